@@ -1,0 +1,135 @@
+/*
+ * tdp1375_b200 — C ABI of the B200 transposition-sequence search and permutation filter.
+ *
+ * The library replaces the native side of the reference's GPUSortingSearch
+ * (src/main/java/br/unb/cic/tdp/base/GPUSortingSearch.java:30-45).  Every entry point
+ * below names the reference function it replaces.  Plain pointers and sizes only:
+ * a JNI, ctypes, cgo or N-API binding can call it directly.
+ *
+ * Threading: tdp_search / tdp_search_batch block the calling thread; different slots
+ * may be used concurrently from different threads (one stream per slot), exactly like
+ * the reference's slot pool.  tdp_cancel may be called from any thread.
+ */
+#ifndef TDP1375_H
+#define TDP1375_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- outcomes (>= 0) and errors (< 0) ----------------------------------------- */
+#define TDP_NOT_FOUND 0        /* no sequence within the ratio/depth (reference: empty array) */
+#define TDP_FOUND 1            /* a sequence was found */
+#define TDP_CANCELLED 2        /* "GPU sorting search cancelled" (sorting_search.cu:841-843) */
+#define TDP_OVERFLOW 3         /* "GPU sorting search queue overflow" (sorting_search.cu:844-846);
+                                  never produced: this engine has no bounded node queue */
+#define TDP_ERR_ARGUMENT (-1)  /* invalid argument (message via tdp_last_error) */
+#define TDP_ERR_SLOT (-2)      /* "invalid slot" */
+#define TDP_ERR_CUDA (-3)      /* CUDA runtime error */
+#define TDP_ERR_OUT_OF_MEMORY (-4)
+#define TDP_ERR_DEVICE (-5)    /* device-side guard tripped (spin limit or deadline) */
+#define TDP_ERR_NOT_INITIALISED (-6)
+
+#define TDP_MAX_N 63     /* MAX_N, core/common.cuh:33-35 */
+#define TDP_MAX_DEPTH 15 /* MAX_DEPTH, core/common.cuh:29-31 */
+
+/* Message of the last failing call on this thread (the text the reference's JNI layer
+ * puts into RuntimeException, jni_sorter.cu:16-23). */
+const char *tdp_last_error(void);
+
+/* Replaces initGpuSortSlots (slot_manager.cu:62-98), JNI initSlots (jni_sorter.cu:25-34).
+ * Destroys previous slots, then creates total_slots slots; slot s lives on device
+ * s % devices_count.  queue_bytes_budget (bytes) bounds the donation pool; dedup_table_size
+ * is the transposition-table capacity in entries (rounded up to a power of two). */
+int tdp_init_slots(int total_slots, int devices_count, int64_t queue_bytes_budget, int dedup_table_size);
+
+/* Replaces destroyGpuSortSlots (slot_manager.cu:22-60), JNI destroySlots (jni_sorter.cu:36-43).
+ * Idempotent. */
+int tdp_destroy_slots(void);
+
+/* Replaces performGpuSortingSearch (sorting_search.cu:701-856) and JNI searchForSortingSeq
+ * (jni_sorter.cu:45-104).  pi/spi are n bytes (read unsigned).  On TDP_FOUND, out_depth
+ * receives d and out_positions 3*d ints: the (i,j,k) positions of each move on the pi array
+ * as it stands before that move (the array GPUSortingSearch.java:65-74 replays).  On
+ * TDP_NOT_FOUND out_depth is 0.  Errors: n > 63, max_moves outside [1,15], spi/pi not
+ * permutations of 0..n-1, bad slot. */
+int tdp_search(int slot, const uint8_t *pi, const uint8_t *spi, int n, int initial_even_cycles, float min_rate,
+               int max_moves, int full_sorting, int32_t *out_positions, int32_t *out_depth);
+
+/* Replaces cancelGpuSort (slot_manager.cu:100-125), JNI cancelSort (jni_sorter.cu:106-109). */
+int tdp_cancel(int slot);
+
+/* Replaces performGpuPiFilter (pi_filter.cu:157-260), JNI filterPiPermutations
+ * (jni_sorter.cu:111-150).  Visits every pi with pi[0]=0 over n symbols and keeps those where
+ * oriented_triple is in cyclic order, cycle is oriented and (unless skip_2move_check) cycle
+ * admits no 2-move.  Writes at most max_rows rows of n bytes to out, in lexicographic order
+ * (the reference's order is arbitrary), and returns the total number of hits (< 0: error). */
+int64_t tdp_pi_filter(const uint8_t *cycle, int cycle_len, const uint8_t *oriented_triple, int triple_len, int n,
+                      int skip_2move_check, uint8_t *out, int64_t max_rows);
+
+/* ---- batched search (no counterpart in the reference; one persistent launch over many
+ *      instances with device-side admission) ---------------------------------------- */
+typedef struct tdp_instance {
+    uint8_t n;
+    uint8_t max_depth;
+    uint8_t full_sorting;
+    uint8_t reserved;
+    int32_t initial_even_cycles;
+    uint8_t pi[64];
+    uint8_t spi[64];
+} tdp_instance; /* 136 bytes */
+
+typedef struct tdp_result {
+    int32_t status;        /* TDP_FOUND / TDP_NOT_FOUND / TDP_CANCELLED / error */
+    int32_t depth;
+    uint64_t nodes;        /* expanded nodes */
+    uint64_t children;     /* children evaluated */
+    int32_t positions[45]; /* 3*depth positions, as tdp_search */
+    int32_t reserved;
+} tdp_result; /* 208 bytes */
+
+int tdp_search_batch(int slot, const tdp_instance *instances, int count, float min_rate, tdp_result *results);
+
+/* Device-resident batch: upload once, run many times, read results. */
+int tdp_batch_prepare(int slot, const tdp_instance *instances, int count, float min_rate);
+int tdp_batch_run(int slot);
+int tdp_batch_results(int slot, tdp_result *results);
+
+/* ---- engine statistics and tuning ---------------------------------------------- */
+typedef struct tdp_stats {
+    uint64_t nodes;
+    uint64_t children;
+    uint64_t dedup_probes;
+    uint64_t dedup_pruned;
+    uint64_t dedup_inserts;
+    uint64_t dedup_full;
+    uint64_t donations;
+    uint64_t task_pops;
+    double kernel_ms;
+    int32_t error;
+    int32_t launches;
+} tdp_stats;
+
+/* Statistics of the last search/batch run on the slot. */
+int tdp_last_stats(int slot, tdp_stats *out);
+
+typedef struct tdp_engine_config {
+    int32_t blocks_per_sm;   /* 0 = occupancy maximum */
+    int32_t poll_interval;   /* chunks between flag polls / donation checks */
+    int32_t tight_bound;     /* 1 = verdict-preserving strengthened prune, 0 = reference prune only */
+    int32_t task_capacity;   /* donation pool entries (<= queue budget) */
+    double time_limit_s;     /* device deadline per launch */
+} tdp_engine_config;
+
+int tdp_get_engine_config(int slot, tdp_engine_config *cfg);
+int tdp_set_engine_config(int slot, const tdp_engine_config *cfg);
+
+int tdp_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TDP1375_H */

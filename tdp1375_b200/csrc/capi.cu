@@ -1,0 +1,232 @@
+// C ABI (include/tdp1375.h): slot table, argument checks, error mapping.
+//
+// Slot management follows slot_manager.cu:22-175 (slot s on device s % devicesCount, one
+// non-blocking stream plus a cancel stream per slot, cancel = host flag + async write of
+// the device flag) and the exception texts of sorting_search.cu:710-715, 841-846 and
+// jni_sorter.cu.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/tdp1375.h"
+#include "pi_filter.h"
+#include "search_engine.h"
+
+namespace {
+
+thread_local std::string gLastError;
+std::mutex gSlotsMutex;
+std::vector<std::shared_ptr<tdp::SearchSlot>> gSlots;
+
+int fail(int code, const std::string &msg) {
+    gLastError = msg;
+    return code;
+}
+
+std::shared_ptr<tdp::SearchSlot> get_slot(int slot) {
+    std::lock_guard<std::mutex> lock(gSlotsMutex);
+    if (slot < 0 || (size_t)slot >= gSlots.size() || !gSlots[slot]) return nullptr;
+    return gSlots[slot];
+}
+
+int map_exception(const std::exception &e) {
+    if (auto *ce = dynamic_cast<const tdp::CudaError *>(&e)) {
+        if (ce->code == cudaErrorMemoryAllocation) return fail(TDP_ERR_OUT_OF_MEMORY, e.what());
+        return fail(TDP_ERR_CUDA, e.what());
+    }
+    if (dynamic_cast<const std::bad_alloc *>(&e)) return fail(TDP_ERR_OUT_OF_MEMORY, "host allocation failed");
+    return fail(TDP_ERR_CUDA, e.what());
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *tdp_last_error(void) { return gLastError.c_str(); }
+
+int tdp_device_count(void) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) return 0;
+    return count;
+}
+
+int tdp_destroy_slots(void) {
+    std::vector<std::shared_ptr<tdp::SearchSlot>> old;
+    {
+        std::lock_guard<std::mutex> lock(gSlotsMutex);
+        old.swap(gSlots);
+    }
+    try {
+        old.clear();
+    } catch (const std::exception &e) {
+        return map_exception(e);
+    }
+    return 0;
+}
+
+int tdp_init_slots(int total_slots, int devices_count, int64_t queue_bytes_budget, int dedup_table_size) {
+    tdp_destroy_slots();
+    if (total_slots <= 0 || devices_count <= 0) return fail(TDP_ERR_ARGUMENT, "initSlots: need at least one slot and one device");
+    int available = tdp_device_count();
+    if (available <= 0) return fail(TDP_ERR_CUDA, "initSlots: no CUDA device");
+    if (devices_count > available) return fail(TDP_ERR_ARGUMENT, "initSlots: devicesCount exceeds the visible devices");
+    int original = -1;
+    cudaGetDevice(&original);
+    std::vector<std::shared_ptr<tdp::SearchSlot>> slots;
+    try {
+        for (int s = 0; s < total_slots; ++s)
+            slots.push_back(std::make_shared<tdp::SearchSlot>(s % devices_count, queue_bytes_budget, dedup_table_size));
+    } catch (const std::exception &e) {
+        if (original >= 0) cudaSetDevice(original);
+        return map_exception(e);
+    }
+    if (original >= 0) cudaSetDevice(original);
+    std::lock_guard<std::mutex> lock(gSlotsMutex);
+    gSlots.swap(slots);
+    return 0;
+}
+
+int tdp_cancel(int slot) {
+    auto s = get_slot(slot);
+    if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    s->cancel();
+    return 0;
+}
+
+int tdp_search_batch(int slot, const tdp_instance *instances, int count, float min_rate, tdp_result *results) {
+    auto s = get_slot(slot);
+    if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    if (count < 0 || (count > 0 && (!instances || !results))) return fail(TDP_ERR_ARGUMENT, "tdp_search_batch: bad buffers");
+    if (count > (1 << tdp::kInstanceBits)) return fail(TDP_ERR_ARGUMENT, "tdp_search_batch: at most 1048576 instances per call");
+    try {
+        std::string err;
+        const int rc = s->searchBatch(instances, count, min_rate, results, err);
+        if (rc != 0) return fail(rc, err);
+        return 0;
+    } catch (const std::exception &e) {
+        return map_exception(e);
+    }
+}
+
+int tdp_search(int slot, const uint8_t *pi, const uint8_t *spi, int n, int initial_even_cycles, float min_rate,
+               int max_moves, int full_sorting, int32_t *out_positions, int32_t *out_depth) {
+    if (out_depth) *out_depth = 0;
+    if (n < 0 || (n > 0 && (!pi || !spi))) return fail(TDP_ERR_ARGUMENT, "performGpuSortingSearch: inconsistent input sizes");
+    if (n > TDP_MAX_N) return fail(TDP_ERR_ARGUMENT, "performGpuSortingSearch: n exceeds MAX_N");
+    if (max_moves <= 0 || max_moves > TDP_MAX_DEPTH)
+        return fail(TDP_ERR_ARGUMENT, "performGpuSortingSearch: invalid maximumDepth");
+    auto s = get_slot(slot);
+    if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    if (n < 3) return TDP_NOT_FOUND;  // no triple: sorting_search.cu:718-719
+    tdp_instance inst;
+    std::memset(&inst, 0, sizeof(inst));
+    inst.n = (uint8_t)n;
+    inst.max_depth = (uint8_t)max_moves;
+    inst.full_sorting = full_sorting ? 1 : 0;
+    inst.initial_even_cycles = initial_even_cycles;
+    std::memcpy(inst.pi, pi, n);
+    std::memcpy(inst.spi, spi, n);
+    tdp_result res;
+    try {
+        std::string err;
+        const int rc = s->searchBatch(&inst, 1, min_rate, &res, err);
+        if (rc != 0) return fail(rc, err);
+    } catch (const std::exception &e) {
+        return map_exception(e);
+    }
+    if (res.status == TDP_CANCELLED) return fail(TDP_CANCELLED, "GPU sorting search cancelled");
+    if (res.status < 0) return fail(res.status, "GPU sorting search did not finish");
+    if (res.status == TDP_FOUND) {
+        if (out_depth) *out_depth = res.depth;
+        if (out_positions) std::memcpy(out_positions, res.positions, sizeof(int32_t) * 3 * res.depth);
+    }
+    return res.status;
+}
+
+int tdp_batch_prepare(int slot, const tdp_instance *instances, int count, float min_rate) {
+    auto s = get_slot(slot);
+    if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    if (count < 0 || (count > 0 && !instances)) return fail(TDP_ERR_ARGUMENT, "tdp_batch_prepare: bad buffers");
+    if (count > (1 << tdp::kInstanceBits)) return fail(TDP_ERR_ARGUMENT, "tdp_batch_prepare: at most 1048576 instances per call");
+    try {
+        std::string err;
+        const int rc = s->stage(instances, count, min_rate, err);
+        if (rc != 0) return fail(rc, err);
+        return 0;
+    } catch (const std::exception &e) {
+        return map_exception(e);
+    }
+}
+
+int tdp_batch_run(int slot) {
+    auto s = get_slot(slot);
+    if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    try {
+        s->clearCancel();
+        std::string err;
+        const int rc = s->runStaged(err);
+        if (rc != 0) return fail(rc, err);
+        return 0;
+    } catch (const std::exception &e) {
+        return map_exception(e);
+    }
+}
+
+int tdp_batch_results(int slot, tdp_result *results) {
+    auto s = get_slot(slot);
+    if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    if (!results && s->stagedCount() > 0) return fail(TDP_ERR_ARGUMENT, "tdp_batch_results: null buffer");
+    try {
+        return s->fetch(results);
+    } catch (const std::exception &e) {
+        return map_exception(e);
+    }
+}
+
+int tdp_last_stats(int slot, tdp_stats *out) {
+    auto s = get_slot(slot);
+    if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    if (out) *out = s->stats();
+    return 0;
+}
+
+int tdp_get_engine_config(int slot, tdp_engine_config *cfg) {
+    auto s = get_slot(slot);
+    if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    if (cfg) *cfg = s->config();
+    return 0;
+}
+
+int tdp_set_engine_config(int slot, const tdp_engine_config *cfg) {
+    auto s = get_slot(slot);
+    if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    if (!cfg || cfg->poll_interval <= 0 || cfg->time_limit_s <= 0 || cfg->blocks_per_sm < 0)
+        return fail(TDP_ERR_ARGUMENT, "tdp_set_engine_config: invalid configuration");
+    s->config() = *cfg;
+    return 0;
+}
+
+int64_t tdp_pi_filter(const uint8_t *cycle, int cycle_len, const uint8_t *oriented_triple, int triple_len, int n,
+                      int skip_2move_check, uint8_t *out, int64_t max_rows) {
+    try {
+        std::string err;
+        const int64_t rc = tdp::pi_filter_run(cycle, cycle_len, oriented_triple, triple_len, n, skip_2move_check, out,
+                                              max_rows, 600.0, err);
+        if (rc >= 0) return rc;
+        switch (rc) {
+            case -1: return fail(TDP_ERR_ARGUMENT, err);
+            case -4: return fail(TDP_ERR_OUT_OF_MEMORY, err);
+            case -5: return fail(TDP_ERR_DEVICE, err);
+            default: return fail(TDP_ERR_CUDA, err);
+        }
+    } catch (const std::exception &e) {
+        return map_exception(e);
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+// Device data layout of the search engine (host and device share these structs).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tdp_math.cuh"
+
+namespace tdp {
+
+// Per-instance state machine (InstanceOut::state).
+enum InstanceState : int {
+    kStatePending = 0,
+    kStateRunning = 1,
+    kStateFound = 2,
+    kStateNotFound = 3,
+};
+
+// One search instance as uploaded by the host (144 B).  spi/pi are the one-line arrays
+// of the reference's JNI call (jni_sorter.cu:45-104, bytes read unsigned).
+struct alignas(16) InstanceIn {
+    uint8_t spi[64];
+    uint8_t pi[64];
+    uint8_t n;
+    uint8_t maxDepth;
+    uint8_t even0;  // odd-length cycles of spi, recounted on the host
+    uint8_t flags;
+    uint32_t rule;  // index into the RuleTable array
+    uint32_t reserved[2];
+};
+
+// Result and live bookkeeping of one instance (96 B).
+struct alignas(16) InstanceOut {
+    int state;        // InstanceState
+    int outstanding;  // tasks of this instance not yet finished
+    int depth;        // solution length when found
+    int reserved;
+    unsigned long long nodes;     // expanded nodes
+    unsigned long long children;  // children evaluated
+    uint32_t moves[16];           // packed positions (pack_triple), depth entries
+};
+
+// A donated piece of work: the children [lo, hi) (lexicographic triple indices) of one
+// node at `depth`, with the move path that reached it (208 B).
+struct alignas(16) Task {
+    uint32_t inst;
+    uint8_t depth;
+    uint8_t even;
+    uint8_t reserved0;
+    uint8_t reserved1;
+    uint16_t lo;
+    uint16_t hi;
+    uint32_t reserved2;
+    uint32_t path[16];
+    uint8_t spi[64];
+    uint8_t pi[64];
+};
+
+enum EngineStat : int {
+    kStatNodes = 0,
+    kStatChildren,
+    kStatDedupProbes,
+    kStatDedupPruned,
+    kStatDedupInserts,
+    kStatDedupFull,
+    kStatDonations,
+    kStatTaskPops,
+    kStatCount
+};
+
+// Launch-wide control block, zeroed before every launch.
+struct EngineCtl {
+    int nextInstance;
+    int doneCount;
+    int hungry;
+    int taskTop;
+    int taskLock;
+    int stop;
+    int error;
+    int reserved;
+    unsigned long long stats[kStatCount];
+};
+
+enum EngineError : int {
+    kErrNone = 0,
+    kErrSpinLimit = 1,
+    kErrDeadline = 2,
+};
+
+constexpr uint32_t kTagWriting = 0xFFFFFFFFu;
+constexpr uint32_t kMaxGeneration = 4094;  // generation 4095 would collide with kTagWriting
+constexpr int kInstanceBits = 20;          // up to 1,048,576 instances per launch
+
+// Transposition-table entry.  key = spi packed 5 bits/symbol, 12 per word (n <= 32) or
+// 6 bits/symbol, 10 per word (n <= 63).  tag = generation << 20 | instance.
+template <int KW>
+struct alignas(KW == 3 ? 32 : 64) DedupEntry {
+    uint32_t tag;
+    uint32_t depth;
+    uint64_t key[KW];
+};
+
+struct EngineParams {
+    const InstanceIn *in;
+    InstanceOut *out;
+    int count;
+    int pollInterval;
+    const RuleTable *rules;
+    const uint32_t *triples;  // lexicographic (i,j,k) per n at offset combinations4(n)
+    void *table;
+    uint32_t tableMask;       // entries - 1 (entries of this launch's layout)
+    uint32_t generation;
+    uint32_t *doneBits;
+    Task *tasks;
+    int taskCap;
+    EngineCtl *ctl;
+    const int *cancel;        // slot cancel flag (device)
+    unsigned long long timeLimitNs;  // every warp stops (error kErrDeadline) after this long
+};
+
+}  // namespace tdp

@@ -1,0 +1,309 @@
+// Permutation filter (replaces pi_filter_kernel / performGpuPiFilter, pi_filter.cu:38-260).
+//
+// Every pi with pi[0] = 0 over n symbols is visited in lexicographic order of
+// pi[1..n-1] (the factoradic rank order of pi_filter.cu:38-53) and kept when
+//   (1) the oriented triple is in cyclic order in pi           (pi_filter.cu:132-133),
+//   (2) the cycle is NOT in cyclic order in pi reversed        (pi_filter.cu:135-142,
+//       CommonOperations.isOriented, CommonOperations.java:443-445),
+//   (3) unless skipped, the cycle admits no 2-move             (pi_filter.cu:86-115,
+//       CommonOperations.java:406-431).
+// B200 layout: each thread walks kRanksPerThread consecutive ranks (one factoradic unrank,
+// then next-permutation steps), so the O(n^2) divisions of the reference happen once per
+// 16 candidates.  Hits are written in rank order: a counting pass stores per-thread hit
+// counts and a block-exclusive prefix, one block scans the block totals, and a writing
+// pass re-evaluates and stores rows at their final offsets.  The reference appends with
+// one atomicAdd per hit in arbitrary order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pi_filter.h"
+
+namespace tdp {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kRanksPerThread = 16;
+constexpr int kRanksPerBlock = kThreads * kRanksPerThread;
+constexpr uint64_t kLaunchRanks = 1ull << 30;
+
+struct FilterArgs {
+    uint8_t cycle[64];
+    uint8_t triple[64];
+    uint8_t cycleIndex[64];
+    unsigned long long fact[21];
+    int cycleLen;
+    int tripleLen;
+    int n;
+    int skip2Move;
+    unsigned long long base;   // first rank of this launch
+    unsigned long long total;  // (n-1)!
+};
+
+__device__ __forceinline__ bool cyclic_order(const uint8_t *index, const uint8_t *symbols, int count) {
+    int leaps = 0;
+    for (int i = 0; i < count; ++i) {
+        const int next = (i + 1 == count) ? 0 : i + 1;
+        if (index[symbols[i]] > index[symbols[next]]) {
+            if (++leaps > 1) return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool cyclic_order3(const uint8_t *index, int a, int b, int c) {
+    const int ia = index[a], ib = index[b], ic = index[c];
+    return ((ia > ib) + (ib > ic) + (ic > ia)) <= 1;
+}
+
+__device__ __forceinline__ int cycle_distance(const uint8_t *cycleIndex, int len, int a, int b) {
+    const int ai = cycleIndex[a], bi = cycleIndex[b];
+    return (bi >= ai) ? bi - ai : (len - ai) + bi;
+}
+
+__device__ bool has_2_move(const FilterArgs &A, const uint8_t *index) {
+    const int len = A.cycleLen;
+    const int before = len & 1;
+    for (int i = 0; i < len - 2; ++i)
+        for (int j = i + 1; j < len - 1; ++j)
+            for (int k = j + 1; k < len; ++k) {
+                const int a = A.cycle[i], b = A.cycle[j], c = A.cycle[k];
+                if (!cyclic_order3(index, a, b, c)) continue;
+                const int after = (cycle_distance(A.cycleIndex, len, a, b) & 1) +
+                                  (cycle_distance(A.cycleIndex, len, b, c) & 1) +
+                                  (cycle_distance(A.cycleIndex, len, c, a) & 1);
+                if (after - before == 2) return true;
+            }
+    return false;
+}
+
+__device__ __forceinline__ void unrank(unsigned long long r, int n, const unsigned long long *fact, uint8_t *p) {
+    uint8_t avail[64];
+    for (int i = 0; i < n - 1; ++i) avail[i] = (uint8_t)(i + 1);
+    p[0] = 0;
+    for (int pos = 0; pos < n - 1; ++pos) {
+        const unsigned long long f = fact[n - 2 - pos];
+        const int choice = (int)(r / f);
+        r -= (unsigned long long)choice * f;
+        p[pos + 1] = avail[choice];
+        for (int q = choice; q < n - 2 - pos; ++q) avail[q] = avail[q + 1];
+    }
+}
+
+__device__ __forceinline__ void next_perm(uint8_t *p, int n) {
+    int i = n - 2;
+    while (i >= 1 && p[i] > p[i + 1]) --i;
+    if (i < 1) return;
+    int j = n - 1;
+    while (p[j] < p[i]) --j;
+    const uint8_t t = p[i];
+    p[i] = p[j];
+    p[j] = t;
+    for (int l = i + 1, r = n - 1; l < r; ++l, --r) {
+        const uint8_t u = p[l];
+        p[l] = p[r];
+        p[r] = u;
+    }
+}
+
+__device__ __forceinline__ bool keep(const FilterArgs &A, const uint8_t *p, uint8_t *index, uint8_t *rindex) {
+    const int n = A.n;
+    for (int i = 0; i < n; ++i) index[p[i]] = (uint8_t)i;
+    if (!cyclic_order(index, A.triple, A.tripleLen)) return false;
+    for (int s = 0; s < n; ++s) rindex[s] = (uint8_t)((n - 1) - index[s]);
+    if (cyclic_order(rindex, A.cycle, A.cycleLen)) return false;
+    if (!A.skip2Move && has_2_move(A, index)) return false;
+    return true;
+}
+
+// Block-wide exclusive scan of one value per thread; returns the prefix, total in *total.
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned *total) {
+    __shared__ unsigned warpSums[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warpSums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned s = (lane < kThreads / 32) ? warpSums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < kThreads / 32) warpSums[lane] = s;
+    }
+    __syncthreads();
+    const unsigned before = (warp > 0 ? warpSums[warp - 1] : 0u) + x - v;
+    *total = warpSums[kThreads / 32 - 1];
+    __syncthreads();
+    return before;
+}
+
+__global__ void __launch_bounds__(kThreads) pi_filter_count_kernel(const FilterArgs A, unsigned *threadPrefix,
+                                                                    unsigned *blockTotal) {
+    uint8_t p[64], index[64], rindex[64];
+    const unsigned long long first =
+        A.base + ((unsigned long long)blockIdx.x * kThreads + threadIdx.x) * kRanksPerThread;
+    unsigned hits = 0;
+    if (first < A.total) {
+        unrank(first, A.n, A.fact, p);
+        const unsigned long long last = min(first + kRanksPerThread, A.total);
+        for (unsigned long long r = first; r < last; ++r) {
+            hits += keep(A, p, index, rindex) ? 1u : 0u;
+            next_perm(p, A.n);
+        }
+    }
+    unsigned total;
+    const unsigned prefix = block_exclusive_scan(hits, &total);
+    threadPrefix[(size_t)blockIdx.x * kThreads + threadIdx.x] = prefix;
+    if (threadIdx.x == 0) blockTotal[blockIdx.x] = total;
+}
+
+// One block: exclusive scan of the block totals (64-bit running offset).
+__global__ void __launch_bounds__(kThreads) pi_filter_scan_kernel(const unsigned *blockTotal,
+                                                                   unsigned long long *blockOffset, int blocks,
+                                                                   unsigned long long *grandTotal) {
+    __shared__ unsigned long long running;
+    if (threadIdx.x == 0) running = *grandTotal;
+    __syncthreads();
+    for (int base = 0; base < blocks; base += kThreads) {
+        const int i = base + (int)threadIdx.x;
+        const unsigned v = (i < blocks) ? blockTotal[i] : 0u;
+        unsigned tileTotal;
+        const unsigned prefix = block_exclusive_scan(v, &tileTotal);
+        if (i < blocks) blockOffset[i] = running + prefix;
+        __syncthreads();
+        if (threadIdx.x == 0) running += tileTotal;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *grandTotal = running;
+}
+
+__global__ void __launch_bounds__(kThreads) pi_filter_write_kernel(const FilterArgs A, const unsigned *threadPrefix,
+                                                                    const unsigned long long *blockOffset,
+                                                                    uint8_t *out, unsigned long long maxRows) {
+    uint8_t p[64], index[64], rindex[64];
+    const unsigned long long first =
+        A.base + ((unsigned long long)blockIdx.x * kThreads + threadIdx.x) * kRanksPerThread;
+    if (first >= A.total) return;
+    unsigned long long row = blockOffset[blockIdx.x] + threadPrefix[(size_t)blockIdx.x * kThreads + threadIdx.x];
+    if (row >= maxRows) return;
+    unrank(first, A.n, A.fact, p);
+    const unsigned long long last = min(first + kRanksPerThread, A.total);
+    for (unsigned long long r = first; r < last && row < maxRows; ++r) {
+        if (keep(A, p, index, rindex)) {
+            uint8_t *dst = out + row * (unsigned long long)A.n;
+            for (int i = 0; i < A.n; ++i) dst[i] = p[i];
+            ++row;
+        }
+        next_perm(p, A.n);
+    }
+}
+
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    ~DeviceBuffer() {
+        if (ptr) cudaFree(ptr);
+    }
+};
+
+bool ok(cudaError_t e, std::string &err, const char *what) {
+    if (e == cudaSuccess) return true;
+    err = std::string(what) + ": CUDA error " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return false;
+}
+
+}  // namespace
+
+int64_t pi_filter_run(const uint8_t *cycle, int cycleLen, const uint8_t *triple, int tripleLen, int n,
+                      int skip2Move, uint8_t *out, int64_t maxRows, double timeLimitS, std::string &err) {
+    if (n > 63) {
+        err = "n exceeds PI_FILTER_MAX_N";
+        return -1;
+    }
+    if (n < 1) {
+        err = "n must be at least 1";
+        return -1;
+    }
+    if (n > 21) {
+        err = "pi filter: (n-1)! does not fit in 64 bits for n > 21";
+        return -1;
+    }
+    if (cycleLen < 0 || cycleLen > 63 || tripleLen < 0 || tripleLen > 63 || maxRows < 0) {
+        err = "pi filter: invalid cycle/triple length or row limit";
+        return -1;
+    }
+    for (int i = 0; i < cycleLen; ++i)
+        if (cycle[i] >= n) {
+            err = "pi filter: cycle symbol out of range";
+            return -1;
+        }
+    for (int i = 0; i < tripleLen; ++i)
+        if (triple[i] >= n) {
+            err = "pi filter: triple symbol out of range";
+            return -1;
+        }
+    FilterArgs A;
+    std::memset(&A, 0, sizeof(A));
+    std::memcpy(A.cycle, cycle, cycleLen);
+    std::memcpy(A.triple, triple, tripleLen);
+    for (int i = 0; i < cycleLen; ++i) A.cycleIndex[cycle[i]] = (uint8_t)i;
+    A.fact[0] = 1;
+    for (int i = 1; i < 21; ++i) A.fact[i] = A.fact[i - 1] * (unsigned long long)i;
+    A.cycleLen = cycleLen;
+    A.tripleLen = tripleLen;
+    A.n = n;
+    A.skip2Move = skip2Move ? 1 : 0;
+    A.total = A.fact[n - 1 > 0 ? n - 1 : 0];
+
+    const uint64_t launchRanks = std::min<uint64_t>(kLaunchRanks, A.total);
+    const int maxBlocks = (int)((launchRanks + kRanksPerBlock - 1) / kRanksPerBlock);
+    DeviceBuffer prefix, totals, offsets, grand, rows;
+    if (!ok(cudaMalloc(&prefix.ptr, (size_t)maxBlocks * kThreads * sizeof(unsigned)), err, "cudaMalloc") ||
+        !ok(cudaMalloc(&totals.ptr, (size_t)maxBlocks * sizeof(unsigned)), err, "cudaMalloc") ||
+        !ok(cudaMalloc(&offsets.ptr, (size_t)maxBlocks * sizeof(unsigned long long)), err, "cudaMalloc") ||
+        !ok(cudaMalloc(&grand.ptr, sizeof(unsigned long long)), err, "cudaMalloc") ||
+        !ok(cudaMemset(grand.ptr, 0, sizeof(unsigned long long)), err, "cudaMemset"))
+        return -3;
+    const size_t outBytes = (size_t)std::max<int64_t>(maxRows, 1) * (size_t)n;
+    if (maxRows > 0 && !ok(cudaMalloc(&rows.ptr, outBytes), err, "cudaMalloc(rows)")) return -4;
+
+    const auto start = std::chrono::steady_clock::now();
+    for (uint64_t base = 0; base < A.total; base += kLaunchRanks) {
+        A.base = base;
+        const uint64_t ranks = std::min<uint64_t>(kLaunchRanks, A.total - base);
+        const int blocks = (int)((ranks + kRanksPerBlock - 1) / kRanksPerBlock);
+        pi_filter_count_kernel<<<blocks, kThreads>>>(A, (unsigned *)prefix.ptr, (unsigned *)totals.ptr);
+        pi_filter_scan_kernel<<<1, kThreads>>>((const unsigned *)totals.ptr, (unsigned long long *)offsets.ptr,
+                                               blocks, (unsigned long long *)grand.ptr);
+        if (maxRows > 0)
+            pi_filter_write_kernel<<<blocks, kThreads>>>(A, (const unsigned *)prefix.ptr,
+                                                         (const unsigned long long *)offsets.ptr,
+                                                         (uint8_t *)rows.ptr, (unsigned long long)maxRows);
+        if (!ok(cudaGetLastError(), err, "pi filter launch")) return -3;
+        if (!ok(cudaDeviceSynchronize(), err, "pi filter")) return -3;
+        const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+        if (base + kLaunchRanks < A.total && elapsed > timeLimitS) {
+            err = "pi filter: time limit exceeded";
+            return -5;
+        }
+    }
+    unsigned long long hits = 0;
+    if (!ok(cudaMemcpy(&hits, grand.ptr, sizeof(hits), cudaMemcpyDeviceToHost), err, "read count")) return -3;
+    const int64_t kept = std::min<int64_t>((int64_t)hits, maxRows);
+    if (kept > 0 && out &&
+        !ok(cudaMemcpy(out, rows.ptr, (size_t)kept * (size_t)n, cudaMemcpyDeviceToHost), err, "read rows"))
+        return -3;
+    return (int64_t)hits;
+}
+
+}  // namespace tdp

@@ -1,0 +1,15 @@
+// Permutation filter host entry (pi_filter.cu).
+#pragma once
+
+#include <stdint.h>
+
+#include <string>
+
+namespace tdp {
+
+// Returns the total number of hits (>= 0) or -1 bad argument, -3 CUDA error,
+// -4 out of memory, -5 time limit; err receives the message.
+int64_t pi_filter_run(const uint8_t *cycle, int cycleLen, const uint8_t *triple, int tripleLen, int n,
+                      int skip2Move, uint8_t *out, int64_t maxRows, double timeLimitS, std::string &err);
+
+}  // namespace tdp

@@ -1,0 +1,395 @@
+// Host runtime of the search engine: per-slot device buffers, rule tables, launches.
+#include "search_engine.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <map>
+#include <vector>
+
+#include "search_kernel.cuh"
+
+namespace tdp {
+
+namespace {
+
+std::mutex gTripleMutex;
+std::vector<uint32_t *> gTriples;  // per device
+
+// Lexicographic (i<j<k) triples for every n in 3..63 at offset C(n,4) (the enumeration
+// order of sorting_search.cu:750-758).
+const uint32_t *device_triples(int device) {
+    std::lock_guard<std::mutex> lock(gTripleMutex);
+    if ((int)gTriples.size() <= device) gTriples.resize(device + 1, nullptr);
+    if (gTriples[device]) return gTriples[device];
+    const int total = combinations4(kMaxN + 1);
+    std::vector<uint32_t> host((size_t)total, 0u);
+    for (int n = 3; n <= kMaxN; ++n) {
+        uint32_t *dst = host.data() + combinations4(n);
+        int t = 0;
+        for (int i = 0; i < n - 2; ++i)
+            for (int j = i + 1; j < n - 1; ++j)
+                for (int k = j + 1; k < n; ++k) dst[t++] = pack_triple(i, j, k);
+    }
+    uint32_t *d = nullptr;
+    check(cudaMalloc(&d, host.size() * sizeof(uint32_t)), "cudaMalloc(triples)");
+    check(cudaMemcpy(d, host.data(), host.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload triples");
+    gTriples[device] = d;
+    return d;
+}
+
+int count_even_host(const uint8_t *spi, int n) {
+    uint64_t seen = 0;
+    int count = 0;
+    for (int s = 0; s < n; ++s) {
+        if ((seen >> s) & 1ull) continue;
+        int size = 0, cur = s;
+        do {
+            seen |= 1ull << cur;
+            ++size;
+            cur = spi[cur];
+        } while (cur != s);
+        count += size & 1;
+    }
+    return count;
+}
+
+bool is_permutation(const uint8_t *a, int n) {
+    uint64_t seen = 0;
+    for (int i = 0; i < n; ++i) {
+        if (a[i] >= n) return false;
+        if ((seen >> a[i]) & 1ull) return false;
+        seen |= 1ull << a[i];
+    }
+    return true;
+}
+
+uint32_t round_pow2(uint64_t v) {
+    uint64_t p = 8;
+    while (p < v && p < (1ull << 31)) p <<= 1;
+    return (uint32_t)p;
+}
+
+}  // namespace
+
+void check(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) throw CudaError(e, what);
+}
+
+SearchSlot::SearchSlot(int device, int64_t queueBytesBudget, int dedupTableSize) : device_(device) {
+    check(cudaSetDevice(device), "cudaSetDevice");
+    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaStreamCreateWithFlags(&cancelStream_, cudaStreamNonBlocking), "cudaStreamCreate(cancel)");
+    check(cudaMalloc(&dCancel_, sizeof(int)), "cudaMalloc(cancel)");
+    check(cudaMemset(dCancel_, 0, sizeof(int)), "cudaMemset(cancel)");
+    check(cudaHostAlloc(&hCancelValue_, sizeof(int), cudaHostAllocPortable), "cudaHostAlloc(cancel)");
+    *hCancelValue_ = 1;
+    check(cudaEventCreate(&evStart_), "cudaEventCreate");
+    check(cudaEventCreate(&evStop_), "cudaEventCreate");
+    triples_ = device_triples(device);
+    check(cudaDeviceGetAttribute(&numSMs_, cudaDevAttrMultiProcessorCount, device), "SM count");
+
+    tableEntries32_ = round_pow2((uint64_t)std::max(dedupTableSize, 1024));
+    check(cudaMalloc(&dTable_, (size_t)tableEntries32_ * 32), "cudaMalloc(dedup table)");
+    check(cudaMemset(dTable_, 0, (size_t)tableEntries32_ * 32), "cudaMemset(dedup table)");
+    const int64_t fromBudget = queueBytesBudget / (int64_t)sizeof(Task);
+    taskCap_ = (int)std::max<int64_t>(1024, std::min<int64_t>(fromBudget, 1 << 16));
+    cfg_.task_capacity = taskCap_;
+    check(cudaMalloc(&dTasks_, (size_t)taskCap_ * sizeof(Task)), "cudaMalloc(tasks)");
+    check(cudaMalloc(&dCtl_, sizeof(EngineCtl)), "cudaMalloc(ctl)");
+    check(cudaHostAlloc(&hCtl_, 2 * sizeof(EngineCtl), cudaHostAllocPortable), "cudaHostAlloc(ctl)");
+    ensureCapacity(1, 1);
+}
+
+SearchSlot::~SearchSlot() {
+    cudaSetDevice(device_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (cancelStream_) cudaStreamSynchronize(cancelStream_);
+    cudaFree(dTable_);
+    cudaFree(dTasks_);
+    cudaFree(dCtl_);
+    cudaFree(dIn_);
+    cudaFree(dOut_);
+    cudaFree(dRules_);
+    cudaFree(dDone_);
+    cudaFree(dCancel_);
+    cudaFreeHost(hCtl_);
+    cudaFreeHost(hIn_);
+    cudaFreeHost(hOut_);
+    cudaFreeHost(hRules_);
+    cudaFreeHost(hCancelValue_);
+    cudaEventDestroy(evStart_);
+    cudaEventDestroy(evStop_);
+    cudaStreamDestroy(stream_);
+    cudaStreamDestroy(cancelStream_);
+}
+
+void SearchSlot::ensureCapacity(int instances, int rules) {
+    if (instances > capInstances_) {
+        const int cap = std::max(instances, capInstances_ * 2);
+        cudaFree(dIn_);
+        cudaFree(dOut_);
+        cudaFree(dDone_);
+        cudaFreeHost(hIn_);
+        cudaFreeHost(hOut_);
+        dIn_ = nullptr;
+        dOut_ = nullptr;
+        dDone_ = nullptr;
+        hIn_ = nullptr;
+        hOut_ = nullptr;
+        check(cudaMalloc(&dIn_, (size_t)cap * sizeof(InstanceIn)), "cudaMalloc(instances)");
+        check(cudaMalloc(&dOut_, (size_t)cap * sizeof(InstanceOut)), "cudaMalloc(results)");
+        check(cudaMalloc(&dDone_, (size_t)((cap + 31) / 32) * sizeof(uint32_t)), "cudaMalloc(done bits)");
+        check(cudaHostAlloc(&hIn_, (size_t)cap * sizeof(InstanceIn), cudaHostAllocPortable), "cudaHostAlloc(in)");
+        check(cudaHostAlloc(&hOut_, (size_t)cap * sizeof(InstanceOut), cudaHostAllocPortable), "cudaHostAlloc(out)");
+        capInstances_ = cap;
+    }
+    if (rules > capRules_) {
+        const int cap = std::max(rules, std::max(64, capRules_ * 2));
+        cudaFree(dRules_);
+        cudaFreeHost(hRules_);
+        dRules_ = nullptr;
+        hRules_ = nullptr;
+        check(cudaMalloc(&dRules_, (size_t)cap * sizeof(RuleTable)), "cudaMalloc(rules)");
+        check(cudaHostAlloc(&hRules_, (size_t)cap * sizeof(RuleTable), cudaHostAllocPortable), "cudaHostAlloc(rules)");
+        capRules_ = cap;
+    }
+}
+
+void SearchSlot::clearCancel() {
+    cancelRequested_.store(false);
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    check(cudaStreamSynchronize(cancelStream_), "sync cancel stream");
+    check(cudaMemsetAsync(dCancel_, 0, sizeof(int), stream_), "reset cancel flag");
+}
+
+void SearchSlot::cancel() {
+    cancelRequested_.store(true);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device_);
+    cudaMemcpyAsync(dCancel_, hCancelValue_, sizeof(int), cudaMemcpyHostToDevice, cancelStream_);
+    if (prev >= 0 && prev != device_) cudaSetDevice(prev);
+}
+
+// Validates and stages instances (n <= 32 first, then n > 32) with their rule tables.
+int SearchSlot::stage(const tdp_instance *instances, int count, float minRate, std::string &err) {
+    order_.clear();
+    order_.reserve(count);
+    for (int pass = 0; pass < 2; ++pass)
+        for (int i = 0; i < count; ++i)
+            if ((instances[i].n > 32) == (pass == 1)) order_.push_back(i);
+    countSmall_ = 0;
+    for (int i = 0; i < count; ++i) countSmall_ += instances[i].n <= 32 ? 1 : 0;
+    count_ = count;
+
+    std::map<std::pair<uint64_t, uint64_t>, uint32_t> ruleIndex;
+    std::vector<RuleTable> rules;
+    ensureCapacity(std::max(count, 1), 1);
+    uint32_t minRateBits;
+    std::memcpy(&minRateBits, &minRate, 4);
+    for (int slotIdx = 0; slotIdx < count; ++slotIdx) {
+        const int src = order_[slotIdx];
+        const tdp_instance &I = instances[src];
+        const int n = I.n;
+        if (n > kMaxN) {
+            err = "performGpuSortingSearch: n exceeds MAX_N";
+            return TDP_ERR_ARGUMENT;
+        }
+        if (I.max_depth <= 0 || I.max_depth > kMaxDepth) {
+            err = "performGpuSortingSearch: invalid maximumDepth";
+            return TDP_ERR_ARGUMENT;
+        }
+        if (!is_permutation(I.spi, n) || !is_permutation(I.pi, n)) {
+            err = "tdp_search: spi and pi must be permutations of 0..n-1 (instance " + std::to_string(src) + ")";
+            return TDP_ERR_ARGUMENT;
+        }
+        const std::pair<uint64_t, uint64_t> key(
+            (uint64_t)n | ((uint64_t)I.max_depth << 8) | ((uint64_t)(I.full_sorting ? 1 : 0) << 16) |
+                ((uint64_t)minRateBits << 32),
+            (uint64_t)(uint32_t)I.initial_even_cycles);
+        auto it = ruleIndex.find(key);
+        uint32_t r;
+        if (it == ruleIndex.end()) {
+            RuleParams p{n, I.initial_even_cycles, I.max_depth, minRate, I.full_sorting ? 1 : 0};
+            r = (uint32_t)rules.size();
+            rules.push_back(build_rule_table(p, cfg_.tight_bound != 0));
+            ruleIndex.emplace(key, r);
+        } else {
+            r = it->second;
+        }
+        InstanceIn &d = hIn_[slotIdx];
+        std::memset(&d, 0, sizeof(d));
+        std::memcpy(d.spi, I.spi, n);
+        std::memcpy(d.pi, I.pi, n);
+        d.n = (uint8_t)n;
+        d.maxDepth = I.max_depth;
+        d.even0 = (uint8_t)count_even_host(I.spi, n);
+        d.rule = r;
+    }
+    ensureCapacity(std::max(count, 1), (int)std::max<size_t>(rules.size(), 1));
+    if (!rules.empty()) std::memcpy(hRules_, rules.data(), rules.size() * sizeof(RuleTable));
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    if (count > 0) {
+        check(cudaMemcpyAsync(dIn_, hIn_, (size_t)count * sizeof(InstanceIn), cudaMemcpyHostToDevice, stream_),
+              "upload instances");
+        check(cudaMemcpyAsync(dRules_, hRules_, rules.size() * sizeof(RuleTable), cudaMemcpyHostToDevice, stream_),
+              "upload rules");
+    }
+    return 0;
+}
+
+void SearchSlot::launchClass(int cls, int offset, int count) {
+    if (count <= 0) return;
+    const int layout = cls;  // 0: 32-byte entries, 1: 64-byte entries
+    if (generation_ >= kMaxGeneration || layout != lastLayout_) {
+        check(cudaMemsetAsync(dTable_, 0, (size_t)tableEntries32_ * 32, stream_), "clear dedup table");
+        generation_ = 0;
+        lastLayout_ = layout;
+    }
+    ++generation_;
+    check(cudaMemsetAsync(dCtl_, 0, sizeof(EngineCtl), stream_), "reset ctl");
+    check(cudaMemsetAsync(dOut_ + offset, 0, (size_t)count * sizeof(InstanceOut), stream_), "reset results");
+    check(cudaMemsetAsync(dDone_, 0, (size_t)((count + 31) / 32) * sizeof(uint32_t), stream_), "reset done bits");
+
+    EngineParams P{};
+    P.in = dIn_ + offset;
+    P.out = dOut_ + offset;
+    P.count = count;
+    P.pollInterval = std::max(1, cfg_.poll_interval);
+    P.rules = dRules_;
+    P.triples = triples_;
+    P.table = dTable_;
+    P.tableMask = (cls == 0 ? tableEntries32_ : tableEntries32_ / 2) - 1u;
+    P.generation = generation_;
+    P.doneBits = dDone_;
+    P.tasks = dTasks_;
+    P.taskCap = std::min(taskCap_, cfg_.task_capacity > 0 ? cfg_.task_capacity : taskCap_);
+    P.ctl = dCtl_;
+    P.cancel = dCancel_;
+    P.timeLimitNs = (unsigned long long)(std::max(0.001, cfg_.time_limit_s) * 1e9);
+
+    int blocksPerSM = 0;
+    const int threads = dev::kWarpsPerBlock * 32;
+    if (cls == 0) {
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocksPerSM, dev::search_engine_kernel<1>, threads, 0),
+              "occupancy");
+    } else {
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocksPerSM, dev::search_engine_kernel<2>, threads, 0),
+              "occupancy");
+    }
+    if (cfg_.blocks_per_sm > 0) blocksPerSM = std::min(blocksPerSM, cfg_.blocks_per_sm);
+    blocksPerSM = std::max(1, blocksPerSM);
+    const int grid = numSMs_ * blocksPerSM;
+    if (cls == 0) {
+        dev::search_engine_kernel<1><<<grid, threads, 0, stream_>>>(P);
+    } else {
+        dev::search_engine_kernel<2><<<grid, threads, 0, stream_>>>(P);
+    }
+    check(cudaGetLastError(), "launch search_engine_kernel");
+    check(cudaMemcpyAsync(hCtl_ + cls, dCtl_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_), "read ctl");
+    launched_[cls] = true;
+    ++launches_;
+}
+
+// Waits for the slot stream while honouring the host cancel request (the device flag
+// was already written by cancel()).
+void SearchSlot::wait() {
+    while (true) {
+        const cudaError_t q = cudaStreamQuery(stream_);
+        if (q == cudaSuccess) return;
+        if (q != cudaErrorNotReady) check(q, "search kernel");
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+int SearchSlot::runStaged(std::string &err) {
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    deviceError_ = 0;
+    launches_ = 0;
+    std::fill(std::begin(statsAccum_), std::end(statsAccum_), 0ull);
+    check(cudaEventRecord(evStart_, stream_), "event");
+    // Both size classes are enqueued back to back; their control blocks are read after.
+    launched_[0] = launched_[1] = false;
+    launchClass(0, 0, countSmall_);
+    launchClass(1, countSmall_, count_ - countSmall_);
+    check(cudaEventRecord(evStop_, stream_), "event");
+    wait();
+    for (int cls = 0; cls < 2; ++cls) {
+        if (!launched_[cls]) continue;
+        const EngineCtl &c = hCtl_[cls];
+        for (int s = 0; s < kStatCount; ++s) statsAccum_[s] += c.stats[s];
+        if (c.error != 0) deviceError_ = c.error;
+    }
+    float ms = 0.f;
+    check(cudaEventElapsedTime(&ms, evStart_, evStop_), "elapsed");
+    kernelMs_ = ms;
+    if (deviceError_ != 0) {
+        err = deviceError_ == kErrDeadline ? "GPU sorting search exceeded its device time limit"
+                                           : "GPU sorting search device error (spin limit)";
+        if (!cancelRequested_.load()) return TDP_ERR_DEVICE;
+    }
+    return 0;
+}
+
+int SearchSlot::fetch(tdp_result *results) {
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    if (count_ > 0) {
+        check(cudaMemcpyAsync(hOut_, dOut_, (size_t)count_ * sizeof(InstanceOut), cudaMemcpyDeviceToHost, stream_),
+              "read results");
+        check(cudaStreamSynchronize(stream_), "sync results");
+    }
+    const bool cancelled = cancelRequested_.load();
+    for (int slotIdx = 0; slotIdx < count_; ++slotIdx) {
+        const InstanceOut &o = hOut_[slotIdx];
+        tdp_result &r = results[order_[slotIdx]];
+        std::memset(&r, 0, sizeof(r));
+        r.nodes = o.nodes;
+        r.children = o.children;
+        if (o.state == kStateFound) {
+            r.status = TDP_FOUND;
+            r.depth = o.depth;
+            for (int d = 0; d < o.depth && d < kMaxDepth; ++d) {
+                r.positions[3 * d] = (int32_t)tri_i(o.moves[d]);
+                r.positions[3 * d + 1] = (int32_t)tri_j(o.moves[d]);
+                r.positions[3 * d + 2] = (int32_t)tri_k(o.moves[d]);
+            }
+        } else if (o.state == kStateNotFound) {
+            r.status = TDP_NOT_FOUND;
+        } else {
+            r.status = cancelled ? TDP_CANCELLED : TDP_ERR_DEVICE;
+        }
+    }
+    return 0;
+}
+
+int SearchSlot::searchBatch(const tdp_instance *instances, int count, float minRate, tdp_result *results,
+                            std::string &err) {
+    clearCancel();
+    int rc = stage(instances, count, minRate, err);
+    if (rc != 0) return rc;
+    rc = runStaged(err);
+    if (rc != 0) return rc;
+    return fetch(results);
+}
+
+tdp_stats SearchSlot::stats() const {
+    tdp_stats s{};
+    s.nodes = statsAccum_[kStatNodes];
+    s.children = statsAccum_[kStatChildren];
+    s.dedup_probes = statsAccum_[kStatDedupProbes];
+    s.dedup_pruned = statsAccum_[kStatDedupPruned];
+    s.dedup_inserts = statsAccum_[kStatDedupInserts];
+    s.dedup_full = statsAccum_[kStatDedupFull];
+    s.donations = statsAccum_[kStatDonations];
+    s.task_pops = statsAccum_[kStatTaskPops];
+    s.kernel_ms = kernelMs_;
+    s.error = deviceError_;
+    s.launches = launches_;
+    return s;
+}
+
+}  // namespace tdp

@@ -1,0 +1,90 @@
+// Host-side search slot: device buffers and launches for one stream on one GPU.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tdp1375.h"
+#include "engine.cuh"
+
+namespace tdp {
+
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t e, const char *what)
+        : std::runtime_error(std::string(what) + ": CUDA error " + cudaGetErrorName(e) + " (" +
+                             cudaGetErrorString(e) + ")"),
+          code(e) {}
+};
+
+void check(cudaError_t e, const char *what);
+
+class SearchSlot {
+public:
+    SearchSlot(int device, int64_t queueBytesBudget, int dedupTableSize);
+    ~SearchSlot();
+    SearchSlot(const SearchSlot &) = delete;
+    SearchSlot &operator=(const SearchSlot &) = delete;
+
+    int device() const { return device_; }
+    void cancel();
+    void clearCancel();
+
+    // Validates + uploads a batch; returns 0 or a TDP_ERR_* code (err holds the message).
+    int stage(const tdp_instance *instances, int count, float minRate, std::string &err);
+    // Runs the staged batch on the device and waits; 0 or TDP_ERR_DEVICE.
+    int runStaged(std::string &err);
+    // Copies the staged batch's results to the caller (in caller order).
+    int fetch(tdp_result *results);
+    int searchBatch(const tdp_instance *instances, int count, float minRate, tdp_result *results, std::string &err);
+
+    tdp_stats stats() const;
+    tdp_engine_config &config() { return cfg_; }
+    int stagedCount() const { return count_; }
+
+private:
+    void ensureCapacity(int instances, int rules);
+    void launchClass(int cls, int offset, int count);
+    void wait();
+
+    int device_ = 0;
+    int numSMs_ = 1;
+    cudaStream_t stream_ = nullptr;
+    cudaStream_t cancelStream_ = nullptr;
+    cudaEvent_t evStart_ = nullptr, evStop_ = nullptr;
+    int *dCancel_ = nullptr;
+    int *hCancelValue_ = nullptr;
+    std::atomic<bool> cancelRequested_{false};
+
+    const uint32_t *triples_ = nullptr;
+    void *dTable_ = nullptr;
+    uint32_t tableEntries32_ = 0;
+    uint32_t generation_ = 0;
+    int lastLayout_ = -1;
+    Task *dTasks_ = nullptr;
+    int taskCap_ = 0;
+    EngineCtl *dCtl_ = nullptr;
+    EngineCtl *hCtl_ = nullptr;  // two snapshots: one per size class
+
+    InstanceIn *dIn_ = nullptr, *hIn_ = nullptr;
+    InstanceOut *dOut_ = nullptr, *hOut_ = nullptr;
+    uint32_t *dDone_ = nullptr;
+    RuleTable *dRules_ = nullptr, *hRules_ = nullptr;
+    int capInstances_ = 0, capRules_ = 0;
+
+    std::vector<int> order_;
+    int count_ = 0, countSmall_ = 0;
+
+    tdp_engine_config cfg_{0, 4, 1, 0, 120.0};
+    unsigned long long statsAccum_[kStatCount] = {};
+    double kernelMs_ = 0.0;
+    int deviceError_ = 0;
+    int launches_ = 0;
+    bool launched_[2] = {false, false};
+};
+
+}  // namespace tdp

@@ -1,0 +1,670 @@
+// Persistent warp-parallel DFS over search instances (device code).
+//
+// Replaces sorting_search_persistent_kernel / initialize_queues_kernel of the reference
+// (sorting_search.cu:377-615) with the same verdict semantics:
+//   * the root (depth 0) is always expanded;
+//   * every child is first tested for success (satisfies_rate, sorting_search.cu:559);
+//   * a child that is not a success is explored only if depth < maxDepth, it passes
+//     can_still_reach and the transposition table admits it (sorting_search.cu:562-563);
+//   * the transposition table prunes a state only when the same state of the same
+//     instance was admitted at a depth <= the current one (sorting_search.cu:261-298);
+//     a full probe window admits without inserting.
+// Layout differences (B200-first, not a translation):
+//   * one warp runs a lazy DFS: a node's children are evaluated 32 at a time (one
+//     lexicographic triple per lane), admitted children are kept as a 32-bit pending
+//     mask and descended into one by one; the frame stack (<= 16 frames) lives in
+//     shared memory (per-lane symbol words) and in lane-indexed registers (frame f's
+//     cursor/mask/key live in lane f), so no node is ever copied through global memory
+//     except when work is donated;
+//   * each lane owns one symbol/position word (spi, pi, cycle leader, steps to leader,
+//     cycle length) so a child's odd-cycle count is an O(1) delta (tdp_math.cuh) instead
+//     of an O(n) recount, and a descent rebuilds the cycle tables with pointer jumping
+//     over warp shuffles;
+//   * idle warps register as hungry; busy warps split the unexplored triple range of
+//     their shallowest frame into a Task in a global pool (work stealing by donation);
+//   * an instance ends when its last task finishes (outstanding counter), so there is
+//     no global termination scan and no queue to overflow;
+//   * the pruning rule is looked up in host-built bit tables (exact float32 semantics);
+//   * table entries carry a (generation, instance) tag so nothing is cleared between
+//     searches; entries of finished instances are reclaimed in place.
+// Every spin has an iteration limit and every loop checks a device deadline, so a bug
+// ends the launch with an error flag instead of hanging the GPU.
+#pragma once
+
+#include "engine.cuh"
+
+namespace tdp {
+namespace dev {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr int kWarpsPerBlock = 8;
+constexpr int kSpinLimit = 1 << 20;
+
+template <int NW>
+struct KeyTraits;
+template <>
+struct KeyTraits<1> {
+    static constexpr int KW = 3, BITS = 5, PER = 12;
+};
+template <>
+struct KeyTraits<2> {
+    static constexpr int KW = 7, BITS = 6, PER = 10;
+};
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_relaxed_s32(const int *p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(uint32_t *p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_time_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <int NW>
+__device__ __forceinline__ uint32_t gather(const uint32_t (&v)[NW], uint32_t idx) {
+    if constexpr (NW == 1) {
+        return __shfl_sync(kFull, v[0], (int)idx);
+    } else {
+        const uint32_t lo = __shfl_sync(kFull, v[0], (int)(idx & 31u));
+        const uint32_t hi = __shfl_sync(kFull, v[1], (int)(idx & 31u));
+        return idx < 32u ? lo : hi;
+    }
+}
+
+__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
+    const uint32_t lo = __shfl_sync(kFull, (uint32_t)v, src);
+    const uint32_t hi = __shfl_sync(kFull, (uint32_t)(v >> 32), src);
+    return ((uint64_t)hi << 32) | lo;
+}
+
+// Rebuilds leader / steps-to-leader / length fields of every word from its spi field.
+template <int NW>
+__device__ __forceinline__ void build_tables(uint32_t (&w)[NW], int n, int lane) {
+    constexpr int R = (NW == 1) ? 5 : 6;
+    uint32_t sv[NW], m[NW], j[NW];
+#pragma unroll
+    for (int h = 0; h < NW; ++h) {
+        const uint32_t x = (uint32_t)(lane + 32 * h);
+        const bool valid = x < (uint32_t)n;
+        sv[h] = w_spi(w[h]);
+        m[h] = x;
+        j[h] = valid ? sv[h] : x;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        uint32_t nm[NW], nj[NW];
+#pragma unroll
+        for (int h = 0; h < NW; ++h) {
+            nm[h] = min(m[h], gather<NW>(m, j[h]));
+            nj[h] = gather<NW>(j, j[h]);
+        }
+#pragma unroll
+        for (int h = 0; h < NW; ++h) {
+            m[h] = nm[h];
+            j[h] = nj[h];
+        }
+    }
+    uint32_t d[NW], p[NW];
+#pragma unroll
+    for (int h = 0; h < NW; ++h) {
+        const uint32_t x = (uint32_t)(lane + 32 * h);
+        const bool sink = (x >= (uint32_t)n) || (x == m[h]);
+        d[h] = sink ? 0u : 1u;
+        p[h] = sink ? x : sv[h];
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        uint32_t nd[NW], np[NW];
+#pragma unroll
+        for (int h = 0; h < NW; ++h) {
+            nd[h] = d[h] + gather<NW>(d, p[h]);
+            np[h] = gather<NW>(p, p[h]);
+        }
+#pragma unroll
+        for (int h = 0; h < NW; ++h) {
+            d[h] = nd[h];
+            p[h] = np[h];
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < NW; ++h) {
+        const uint32_t afterLeader = gather<NW>(sv, m[h]);
+        const uint32_t len = gather<NW>(d, afterLeader) + 1u;
+        const uint32_t x = (uint32_t)(lane + 32 * h);
+        w[h] = (x < (uint32_t)n) ? w_make(sv[h], w_pi(w[h]), m[h], d[h], len) : 0u;
+    }
+}
+
+template <int NW>
+__device__ __forceinline__ void compute_key(const uint32_t (&w)[NW], int n, int lane,
+                                            uint64_t (&key)[KeyTraits<NW>::KW]) {
+    using K = KeyTraits<NW>;
+#pragma unroll
+    for (int q = 0; q < K::KW; ++q) {
+        uint64_t c = 0;
+#pragma unroll
+        for (int h = 0; h < NW; ++h) {
+            const int x = lane + 32 * h;
+            if (x < n && x / K::PER == q) c |= (uint64_t)w_spi(w[h]) << (K::BITS * (x % K::PER));
+        }
+        const uint32_t lo = __reduce_or_sync(kFull, (uint32_t)c);
+        const uint32_t hi = __reduce_or_sync(kFull, (uint32_t)(c >> 32));
+        key[q] = ((uint64_t)hi << 32) | lo;
+    }
+}
+
+template <int NW>
+__device__ __forceinline__ void set_field(uint64_t (&key)[KeyTraits<NW>::KW], uint32_t x, uint32_t v) {
+    using K = KeyTraits<NW>;
+    const uint32_t q = x / K::PER;
+    const uint32_t s = K::BITS * (x - q * K::PER);
+    const uint64_t mask = ((1ull << K::BITS) - 1ull) << s;
+    const uint64_t val = (uint64_t)v << s;
+#pragma unroll
+    for (int qq = 0; qq < K::KW; ++qq)
+        if (qq == (int)q) key[qq] = (key[qq] & ~mask) | val;
+}
+
+template <int KW>
+__device__ __forceinline__ uint64_t key_hash(const uint64_t (&k)[KW], uint32_t tag) {
+    uint64_t h = 0x9E3779B97F4A7C15ull ^ ((uint64_t)tag << 17);
+#pragma unroll
+    for (int q = 0; q < KW; ++q) {
+        h ^= k[q];
+        h *= 0xBF58476D1CE4E5B9ull;
+        h ^= h >> 29;
+    }
+    h *= 0x94D049BB133111EBull;
+    h ^= h >> 32;
+    return h;
+}
+
+struct LaneStats {
+    unsigned long long probes = 0, pruned = 0, inserts = 0, full = 0;
+};
+
+__device__ __forceinline__ bool tag_reclaimable(const EngineParams &P, uint32_t t) {
+    if (t == 0u) return true;
+    if ((t >> kInstanceBits) != P.generation) return true;
+    const uint32_t idx = t & ((1u << kInstanceBits) - 1u);
+    return (ld_relaxed_u32(P.doneBits + (idx >> 5)) >> (idx & 31u)) & 1u;
+}
+
+// Transposition-table admission (sorting_search.cu:261-298 semantics, per instance).
+template <int KW>
+__device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t tag, const uint64_t (&key)[KW],
+                                            uint64_t h, uint32_t depth, LaneStats &ls) {
+    auto *table = reinterpret_cast<DedupEntry<KW> *>(P.table);
+    const uint32_t base = (uint32_t)(h >> 24) & P.tableMask & ~7u;
+    ++ls.probes;
+    uint32_t tags[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) tags[q] = ld_acquire_u32(&table[base + q].tag);
+    int freeSlot = -1;
+    uint32_t freeTag = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const uint32_t t = tags[q];
+        if (t == tag) {
+            DedupEntry<KW> *e = &table[base + q];
+            bool eq = true;
+#pragma unroll
+            for (int kq = 0; kq < KW; ++kq) eq &= (__ldcg(&e->key[kq]) == key[kq]);
+            if (eq) {
+                const uint32_t prev = atomicMin(&e->depth, depth);
+                if (prev <= depth) {
+                    ++ls.pruned;
+                    return false;
+                }
+                return true;
+            }
+        } else if (freeSlot < 0 && t != kTagWriting && tag_reclaimable(P, t)) {
+            freeSlot = q;
+            freeTag = t;
+        }
+    }
+    if (freeSlot >= 0) {
+        DedupEntry<KW> *e = &table[base + freeSlot];
+        if (atomicCAS(&e->tag, freeTag, kTagWriting) == freeTag) {
+            e->depth = depth;
+#pragma unroll
+            for (int kq = 0; kq < KW; ++kq) __stcg(&e->key[kq], key[kq]);
+            __threadfence();
+            st_release_u32(&e->tag, tag);
+            ++ls.inserts;
+        }
+    } else {
+        ++ls.full;
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool lock_acquire(EngineCtl *ctl) {
+    for (int it = 0; it < kSpinLimit; ++it) {
+        if (atomicCAS(&ctl->taskLock, 0, 1) == 0) {
+            __threadfence();
+            return true;
+        }
+        __nanosleep(64);
+    }
+    atomicExch(&ctl->error, kErrSpinLimit);
+    atomicExch(&ctl->stop, 1);
+    return false;
+}
+
+__device__ __forceinline__ void lock_release(EngineCtl *ctl) {
+    __threadfence();
+    atomicExch(&ctl->taskLock, 0);
+}
+
+template <int NW>
+struct WarpShared {
+    uint32_t words[kMaxDepth + 1][NW * 32];
+    uint32_t staging[52];
+};
+
+template <int NW>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(const EngineParams P) {
+    using K = KeyTraits<NW>;
+    constexpr int KW = K::KW;
+    __shared__ WarpShared<NW> smem[kWarpsPerBlock];
+    const int lane = (int)(threadIdx.x & 31u);
+    WarpShared<NW> &S = smem[threadIdx.x >> 5];
+    EngineCtl *ctl = P.ctl;
+    const unsigned long long deadline = global_time_ns() + P.timeLimitNs;
+
+    unsigned long long wNodes = 0, wChildren = 0, wDonations = 0, wPops = 0;
+    LaneStats ls;
+    bool hungry = false;
+    int backoff = 32;
+    bool stopAll = false;
+
+    while (!stopAll) {
+        // ---------------------------------------------------------------- get work
+        int kind = 0, idx = 0;
+        if (lane == 0) {
+            if (ld_relaxed_s32(&ctl->stop) || ld_relaxed_s32(P.cancel) || global_time_ns() > deadline) {
+                if (global_time_ns() > deadline) {
+                    atomicExch(&ctl->error, kErrDeadline);
+                    atomicExch(&ctl->stop, 1);
+                }
+                kind = -1;
+            } else {
+                if (ld_relaxed_s32(&ctl->taskTop) > 0) {
+                    if (lock_acquire(ctl)) {
+                        volatile int *top = &ctl->taskTop;
+                        const int t = *top;
+                        if (t > 0) {
+                            *top = t - 1;
+                            idx = t - 1;
+                            kind = 1;
+                        } else {
+                            lock_release(ctl);
+                        }
+                    } else {
+                        kind = -1;
+                    }
+                }
+                if (kind == 0 && ld_relaxed_s32(&ctl->nextInstance) < P.count) {
+                    const int i = atomicAdd(&ctl->nextInstance, 1);
+                    if (i < P.count) {
+                        kind = 2;
+                        idx = i;
+                    }
+                }
+                if (kind == 0 && ld_relaxed_s32(&ctl->doneCount) >= P.count) kind = -1;
+            }
+        }
+        kind = __shfl_sync(kFull, kind, 0);
+        idx = __shfl_sync(kFull, idx, 0);
+        if (kind < 0) break;
+        if (kind == 0) {
+            if (!hungry && lane == 0) atomicAdd(&ctl->hungry, 1);
+            hungry = true;
+            __nanosleep(backoff);
+            backoff = min(backoff * 2, 4096);
+            continue;
+        }
+        if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
+        hungry = false;
+        backoff = 32;
+
+        // ---------------------------------------------------------------- set up
+        uint32_t inst;
+        int baseDepth, even, lo, hi;
+        uint32_t w[NW];
+        uint32_t fMove = 0;
+        unsigned long long tNodes = 0, tChildren = 0;
+        if (kind == 1) {
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(P.tasks + idx);
+            for (int q = lane; q < 52; q += 32) S.staging[q] = __ldcg(src + q);
+            __syncwarp();
+            if (lane == 0) lock_release(ctl);
+            ++wPops;
+            inst = S.staging[0];
+            baseDepth = (int)(S.staging[1] & 0xFFu);
+            even = (int)((S.staging[1] >> 8) & 0xFFu);
+            lo = (int)(S.staging[2] & 0xFFFFu);
+            hi = (int)(S.staging[2] >> 16);
+            if (lane < baseDepth) fMove = S.staging[4 + lane];
+            const uint8_t *bytes = reinterpret_cast<const uint8_t *>(S.staging);
+            const int n = P.in[inst].n;
+#pragma unroll
+            for (int h = 0; h < NW; ++h) {
+                const int x = lane + 32 * h;
+                w[h] = (x < n) ? ((uint32_t)bytes[80 + x] | ((uint32_t)bytes[144 + x] << 6)) : 0u;
+            }
+            __syncwarp();
+        } else {
+            inst = (uint32_t)idx;
+            const InstanceIn *I = P.in + inst;
+            if (lane == 0) {
+                atomicExch(&P.out[inst].outstanding, 1);
+                atomicExch(&P.out[inst].state, kStateRunning);
+            }
+            baseDepth = 0;
+            even = I->even0;
+            lo = 0;
+            hi = combinations3(I->n);
+            const int n = I->n;
+#pragma unroll
+            for (int h = 0; h < NW; ++h) {
+                const int x = lane + 32 * h;
+                w[h] = (x < n) ? ((uint32_t)I->spi[x] | ((uint32_t)I->pi[x] << 6)) : 0u;
+            }
+            tNodes = 1;
+        }
+        const int n = P.in[inst].n;
+        const int T = combinations3(n);
+        const uint32_t *trip = P.triples + combinations4(n);
+        const uint32_t tag = (P.generation << kInstanceBits) | inst;
+        const RuleTable *rt = P.rules + P.in[inst].rule;
+        const uint64_t ruleReg = (lane < 16) ? rt->sat[lane] : rt->expand[lane - 16];
+
+        build_tables<NW>(w, n, lane);
+        uint64_t key[KW];
+        compute_key<NW>(w, n, lane, key);
+
+        int f = baseDepth;
+        int cursor = lo, end = hi, chunk = 0;
+        uint32_t pending = 0;
+        int fCursor = 0, fEnd = 0, fChunk = 0, fEven = 0;
+        uint32_t fPending = 0;
+        uint64_t fKey[KW];
+#pragma unroll
+        for (int q = 0; q < KW; ++q) fKey[q] = 0;
+#pragma unroll
+        for (int h = 0; h < NW; ++h) S.words[f][h * 32 + lane] = w[h];
+        uint64_t satMask = shfl64(ruleReg, f + 1);
+        uint64_t expMask = shfl64(ruleReg, 16 + f + 1);
+
+        // outcome: 0 subtree exhausted, 1 instance found (here or elsewhere), 2 launch stop
+        int outcome = 0;
+        if (kind == 1) {
+            int st = 0;
+            if (lane == 0) st = ld_relaxed_s32(&P.out[inst].state);
+            if (__shfl_sync(kFull, st, 0) == kStateFound) outcome = 1;
+        }
+        int poll = 0;
+        while (outcome == 0) {
+            if (pending == 0u) {
+                if (cursor >= end) {
+                    if (f == baseDepth) break;
+                    --f;
+                    cursor = __shfl_sync(kFull, fCursor, f);
+                    end = __shfl_sync(kFull, fEnd, f);
+                    pending = __shfl_sync(kFull, fPending, f);
+                    chunk = __shfl_sync(kFull, fChunk, f);
+                    even = __shfl_sync(kFull, fEven, f);
+#pragma unroll
+                    for (int q = 0; q < KW; ++q) key[q] = shfl64(fKey[q], f);
+#pragma unroll
+                    for (int h = 0; h < NW; ++h) w[h] = S.words[f][h * 32 + lane];
+                    satMask = shfl64(ruleReg, f + 1);
+                    expMask = shfl64(ruleReg, 16 + f + 1);
+                    continue;
+                }
+                if (++poll >= P.pollInterval) {
+                    poll = 0;
+                    int act = 0;
+                    if (lane == 0) {
+                        if (ld_relaxed_s32(&ctl->stop) || ld_relaxed_s32(P.cancel)) {
+                            act = 2;
+                        } else if (global_time_ns() > deadline) {
+                            atomicExch(&ctl->error, kErrDeadline);
+                            atomicExch(&ctl->stop, 1);
+                            act = 2;
+                        } else if (ld_relaxed_s32(&P.out[inst].state) == kStateFound) {
+                            act = 1;
+                        } else {
+                            const int hg = ld_relaxed_s32(&ctl->hungry);
+                            if (hg > 0 && ld_relaxed_s32(&ctl->taskTop) < hg) act = 3;
+                        }
+                    }
+                    act = __shfl_sync(kFull, act, 0);
+                    if (act == 1 || act == 2) {
+                        outcome = act;
+                        break;
+                    }
+                    if (act == 3) {
+                        // ------------------------------------------------ donate
+                        int rem = 0;
+                        if (lane >= baseDepth && lane < f) rem = fEnd - fCursor;
+                        if (lane == f) rem = end - cursor;
+                        const unsigned big = __ballot_sync(kFull, rem >= 64);
+                        const unsigned some = __ballot_sync(kFull, rem > 0 && lane < f);
+                        const int g = big ? (__ffs(big) - 1) : (some ? (__ffs(some) - 1) : -1);
+                        if (g >= 0) {
+                            const int gc = __shfl_sync(kFull, (lane == f) ? cursor : fCursor, g);
+                            const int ge = __shfl_sync(kFull, (lane == f) ? end : fEnd, g);
+                            const int gEven = __shfl_sync(kFull, (lane == f) ? even : fEven, g);
+                            const int remg = ge - gc;
+                            const int keepChunks = (remg >= 64) ? (((remg + 31) / 32 + 1) / 2) : 0;
+                            const int newEnd = min(ge, gc + keepChunks * 32);
+                            int slot = -1;
+                            if (lane == 0 && newEnd < ge) {
+                                atomicAdd(&P.out[inst].outstanding, 1);
+                                if (lock_acquire(ctl)) {
+                                    volatile int *top = &ctl->taskTop;
+                                    if (*top < P.taskCap) {
+                                        slot = *top;
+                                    } else {
+                                        lock_release(ctl);
+                                    }
+                                }
+                                if (slot < 0) atomicSub(&P.out[inst].outstanding, 1);
+                            }
+                            slot = __shfl_sync(kFull, slot, 0);
+                            if (slot >= 0) {
+                                Task *tk = P.tasks + slot;
+                                if (lane == 0) {
+                                    uint32_t *hdr = reinterpret_cast<uint32_t *>(tk);
+                                    hdr[0] = inst;
+                                    hdr[1] = (uint32_t)g | ((uint32_t)gEven << 8);
+                                    hdr[2] = (uint32_t)newEnd | ((uint32_t)ge << 16);
+                                    hdr[3] = 0u;
+                                }
+                                if (lane < g) tk->path[lane] = fMove;
+#pragma unroll
+                                for (int h = 0; h < NW; ++h) {
+                                    const int x = lane + 32 * h;
+                                    if (x < n) {
+                                        const uint32_t wg = S.words[g][h * 32 + lane];
+                                        tk->spi[x] = (uint8_t)w_spi(wg);
+                                        tk->pi[x] = (uint8_t)w_pi(wg);
+                                    }
+                                }
+                                __threadfence();
+                                __syncwarp();
+                                if (lane == 0) {
+                                    volatile int *top = &ctl->taskTop;
+                                    *top = slot + 1;
+                                    lock_release(ctl);
+                                }
+                                if (g == f) {
+                                    end = newEnd;
+                                } else if (lane == g) {
+                                    fEnd = newEnd;
+                                }
+                                ++wDonations;
+                            }
+                        }
+                        // The donor keeps at least one chunk of its current frame
+                        // (newEnd > cursor when g == f), so it evaluates it next.
+                    }
+                }
+                // ---------------------------------------------------- evaluate a chunk
+                chunk = cursor;
+                const int t = cursor + lane;
+                cursor += 32;
+                const bool valid = t < end;
+                const uint32_t tr = valid ? __ldg(trip + t) : 0u;
+                const uint32_t a = w_pi(gather<NW>(w, tri_i(tr)));
+                const uint32_t b = w_pi(gather<NW>(w, tri_j(tr)));
+                const uint32_t c = w_pi(gather<NW>(w, tri_k(tr)));
+                const uint32_t wa = gather<NW>(w, a);
+                const uint32_t wb = gather<NW>(w, b);
+                const uint32_t wc = gather<NW>(w, c);
+                const int e = even + move_delta(wa, wb, wc);
+                const bool sat = valid && ((satMask >> e) & 1ull);
+                tChildren += (unsigned long long)min(32, end - chunk);
+                const unsigned satBallot = __ballot_sync(kFull, sat);
+                if (satBallot) {
+                    const int winner = __ffs(satBallot) - 1;
+                    const uint32_t wtr = __shfl_sync(kFull, tr, winner);
+                    int won = 0;
+                    if (lane == 0) won = atomicCAS(&P.out[inst].state, kStateRunning, kStateFound) == kStateRunning;
+                    won = __shfl_sync(kFull, won, 0);
+                    if (won) {
+                        if (lane < f) P.out[inst].moves[lane] = fMove;
+                        if (lane == f) {
+                            P.out[inst].moves[f] = wtr;
+                            P.out[inst].depth = f + 1;
+                        }
+                        __threadfence();
+                    }
+                    outcome = 1;
+                    break;
+                }
+                bool adm = valid && ((expMask >> e) & 1ull);
+                if (adm) {
+                    uint64_t ck[KW];
+#pragma unroll
+                    for (int q = 0; q < KW; ++q) ck[q] = key[q];
+                    set_field<NW>(ck, a, w_spi(wc));
+                    set_field<NW>(ck, b, w_spi(wa));
+                    set_field<NW>(ck, c, w_spi(wb));
+                    adm = dedup_admit<KW>(P, tag, ck, key_hash<KW>(ck, tag), (uint32_t)(f + 1), ls);
+                }
+                pending = __ballot_sync(kFull, adm);
+                continue;
+            }
+            // -------------------------------------------------------- descend
+            const int l = __ffs(pending) - 1;
+            pending &= pending - 1u;
+            const uint32_t tr = __ldg(trip + chunk + l);
+            if (lane == f) {
+                fCursor = cursor;
+                fEnd = end;
+                fPending = pending;
+                fChunk = chunk;
+                fEven = even;
+                fMove = tr;
+#pragma unroll
+                for (int q = 0; q < KW; ++q) fKey[q] = key[q];
+            }
+            const uint32_t i = tri_i(tr), j = tri_j(tr), k = tri_k(tr);
+            const uint32_t a = w_pi(gather<NW>(w, i));
+            const uint32_t b = w_pi(gather<NW>(w, j));
+            const uint32_t c = w_pi(gather<NW>(w, k));
+            const uint32_t wa = gather<NW>(w, a);
+            const uint32_t wb = gather<NW>(w, b);
+            const uint32_t wc = gather<NW>(w, c);
+            even += move_delta(wa, wb, wc);
+            set_field<NW>(key, a, w_spi(wc));
+            set_field<NW>(key, b, w_spi(wa));
+            set_field<NW>(key, c, w_spi(wb));
+            uint32_t nw[NW];
+#pragma unroll
+            for (int h = 0; h < NW; ++h) {
+                const uint32_t x = (uint32_t)(lane + 32 * h);
+                uint32_t s = w_spi(w[h]);
+                if (x == a) s = w_spi(wc);
+                if (x == b) s = w_spi(wa);
+                if (x == c) s = w_spi(wb);
+                const uint32_t src = (uint32_t)block_swap_src((int)x, (int)i, (int)j, (int)k);
+                nw[h] = s | (w_pi(gather<NW>(w, src)) << 6);
+            }
+#pragma unroll
+            for (int h = 0; h < NW; ++h) w[h] = nw[h];
+            build_tables<NW>(w, n, lane);
+            ++f;
+#pragma unroll
+            for (int h = 0; h < NW; ++h) S.words[f][h * 32 + lane] = w[h];
+            cursor = 0;
+            end = T;
+            pending = 0u;
+            satMask = shfl64(ruleReg, f + 1);
+            expMask = shfl64(ruleReg, 16 + f + 1);
+            ++tNodes;
+        }
+        wNodes += tNodes;
+        wChildren += tChildren;
+        if (outcome == 2) {
+            stopAll = true;
+            break;
+        }
+        // ---------------------------------------------------------------- finish task
+        if (lane == 0) {
+            atomicAdd(&P.out[inst].nodes, tNodes);
+            atomicAdd(&P.out[inst].children, tChildren);
+            const int prev = atomicSub(&P.out[inst].outstanding, 1);
+            if (prev == 1) {
+                atomicCAS(&P.out[inst].state, kStateRunning, kStateNotFound);
+                atomicOr(P.doneBits + (inst >> 5), 1u << (inst & 31u));
+                __threadfence();
+                atomicAdd(&ctl->doneCount, 1);
+            }
+        }
+        __syncwarp();
+    }
+    if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
+
+    // ---------------------------------------------------------------- statistics
+    unsigned long long probes = ls.probes, pruned = ls.pruned, inserts = ls.inserts, full = ls.full;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        probes += __shfl_xor_sync(kFull, probes, o);
+        pruned += __shfl_xor_sync(kFull, pruned, o);
+        inserts += __shfl_xor_sync(kFull, inserts, o);
+        full += __shfl_xor_sync(kFull, full, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&ctl->stats[kStatNodes], wNodes);
+        atomicAdd(&ctl->stats[kStatChildren], wChildren);
+        atomicAdd(&ctl->stats[kStatDedupProbes], probes);
+        atomicAdd(&ctl->stats[kStatDedupPruned], pruned);
+        atomicAdd(&ctl->stats[kStatDedupInserts], inserts);
+        atomicAdd(&ctl->stats[kStatDedupFull], full);
+        atomicAdd(&ctl->stats[kStatDonations], wDonations);
+        atomicAdd(&ctl->stats[kStatTaskPops], wPops);
+    }
+}
+
+}  // namespace dev
+}  // namespace tdp
