@@ -1,0 +1,367 @@
+"""Benchmark: cases resolved/s (and nodes/s) of the transposition-sequence search on B200.
+
+Workload: 3-permutation configurations of the tdp1375 proof (spi = product of m disjoint
+3-cycles on n = 3m symbols, pi = identity), m ~ U{4..8}, seeded case by case
+(seed 1375 + 2*10**6 + case) over a 100,000-case set; full sorting, ratio 1.375
+(minRate = float32(2)/float32(1.375)), max depth 11, transposition table of 2M entries,
+queue budget 3000 MB, one slot.  A step is one batch of --batch consecutive cases
+(step s of rank r covers cases [(s*N + r)*B, (s*N + r + 1)*B) mod 100,000).
+
+value: cases/s with the step's instances already resident in HBM (tdp_batch_prepare before
+the timed region; tdp_batch_run timed with CUDA events on the engine's stream), L2 flushed
+with a 256 MB write between steps.  e2e: the same steps through tdp_search_batch with host
+buffers (upload, run, download inside the timed region).  --impl reference times the CPU
+restatement of the reference's CPU search (SortingSearch.java) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TOTAL_CASES = 100_000
+CONFIG = 2
+MAX_DEPTH = 11
+DEDUP_ENTRIES = 1 << 21
+QUEUE_BYTES = 3000 << 20
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--batch", type=int, default=2000)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--cpu-budget-s", type=float, default=15.0, help="CPU baseline sample length")
+    p.add_argument("--cpu-node-limit", type=int, default=3_000_000)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", choices=["config2", "config1"], default="config2",
+                   help="config1 (m~U{4,5,6}) is the small case used for profiling")
+    p.add_argument("--table-entries", type=int, default=DEDUP_ENTRIES)
+    p.add_argument("--time-limit-s", type=float, default=600.0)
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def step_cases(step: int, rank: int, world: int, batch: int, config: int = CONFIG):
+    from tdp1375_b200.cases import config_cases
+    start = ((step * world + rank) * batch) % TOTAL_CASES
+    out = []
+    for case in range(start, start + batch):
+        c = next(config_cases(config, 1, start=case % TOTAL_CASES))
+        out.append(c)
+    return out
+
+
+# ------------------------------------------------------------------------- CPU baseline
+def _cpu_solve(args):
+    case, node_limit = args
+    import numpy as np  # noqa: F401
+    from oracle import oracle as O
+    from tdp1375_b200.cases import config_cases, MIN_RATE
+    pi, spi, even, m = next(config_cases(CONFIG, 1, start=case))
+    t = time.perf_counter()
+    st, _, expanded = O.search_cpu_rule(list(pi), list(spi), even, float(MIN_RATE), MAX_DEPTH, node_limit=node_limit)
+    return case, st, expanded, time.perf_counter() - t
+
+
+def cpu_sample(budget_s: float, node_limit: int, first_case: int = 0):
+    """Runs the SortingSearch.java restatement over consecutive cases on all host cores for
+    about budget_s seconds.  Returns (resolved cases/s, expanded nodes/s, cores, detail)."""
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    resolved = 0
+    nodes = 0
+    submitted = 0
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        pending = []
+        case = first_case
+        while True:
+            while len(pending) < 2 * cores:
+                pending.append(pool.apply_async(_cpu_solve, ((case % TOTAL_CASES, node_limit),)))
+                case += 1
+                submitted += 1
+            done = [p for p in pending if p.ready()]
+            for p in done:
+                pending.remove(p)
+                _, st, expanded, _ = p.get()
+                nodes += expanded
+                if st in (0, 1):
+                    resolved += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+            time.sleep(0.01)
+        elapsed = time.perf_counter() - t0
+        pool.terminate()
+    detail = (f"SortingSearch.java restatement (oracle port), {cores} processes, consecutive config-2 cases from "
+              f"{first_case} for {elapsed:.1f} s, per-case limit {node_limit} expanded nodes; {resolved} resolved")
+    return resolved / elapsed, nodes / elapsed, cores, detail
+
+
+# ------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        import statistics
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[2:6]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------- GPU arm
+def measured_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def algorithmic_bytes(stats, instances: int) -> float:
+    """Bytes the search must move per launch: every transposition-table probe touches a window
+    of 8 entries (8 sectors of 32 B), every insert writes one 32 B entry, every donated task
+    is written and read once (2 x 208 B), every instance is read (144 B) and written (96 B)."""
+    return 256.0 * stats.dedup_probes + 32.0 * stats.dedup_inserts + 416.0 * stats.donations + 240.0 * instances
+
+
+def run_ours(args):
+    import ctypes
+
+    import torch
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    from tdp1375_b200 import GPUSortingSearch, api, make_instances, native
+
+    lib = native.load()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(args.cpu_budget_s, args.cpu_node_limit)
+
+    GPUSortingSearch(1, 1, QUEUE_BYTES, args.table_entries)  # slot 0 on the current device
+    cfg = api.engine_config(0)
+    cfg.time_limit_s = args.time_limit_s
+    api.set_engine_config(0, cfg)
+    config_id = 1 if args.workload == "config1" else CONFIG
+    flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")
+    total_steps = args.warmup + args.steps
+
+    batches = [make_instances([c[:3] for c in step_cases(s, rank, world, args.batch, config_id)], MAX_DEPTH, True)
+               for s in range(total_steps)]
+    rate = ctypes.c_float(float(__import__("numpy").float32(2) / __import__("numpy").float32(1.375)))
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident value
+    kernel_ms = []
+    stats = []
+    found = notfound = other = 0
+    with ClockSampler(local) as clocks:
+        for s in range(total_steps):
+            if lib.tdp_batch_prepare(0, batches[s], args.batch, rate) != 0:
+                raise RuntimeError(native.last_error())
+            flush.fill_(s)
+            barrier()
+            if lib.tdp_batch_run(0) != 0:
+                raise RuntimeError(native.last_error())
+            st = api.last_stats(0)
+            barrier()
+            if s >= args.warmup:
+                kernel_ms.append(st.kernel_ms)
+                stats.append((st.nodes, st.children, st.dedup_probes, st.dedup_inserts, st.donations, st.launches))
+                res = (native.Result * args.batch)()
+                lib.tdp_batch_results(0, res)
+                for r in res:
+                    if r.status == native.FOUND:
+                        found += 1
+                    elif r.status == native.NOT_FOUND:
+                        notfound += 1
+                    else:
+                        other += 1
+    device_s = sum(kernel_ms) / 1e3
+    if world > 1:
+        t = torch.tensor([device_s], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        device_s = float(t.item())
+    cases = args.batch * args.steps * world
+    value = cases / device_s
+    nodes = sum(x[0] for x in stats)
+
+    # ---- e2e through the C ABI with host buffers
+    wall = 0.0
+    results = (native.Result * args.batch)()
+    for s in range(0 if args.no_e2e else total_steps):
+        flush.fill_(s)
+        barrier()
+        t0 = time.perf_counter()
+        if lib.tdp_search_batch(0, batches[s], args.batch, rate, results) != 0:
+            raise RuntimeError(native.last_error())
+        dt = time.perf_counter() - t0
+        barrier()
+        if s >= args.warmup:
+            wall += dt
+    if world > 1:
+        t = torch.tensor([wall], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        wall = float(t.item())
+
+    # ---- roofline of the search kernel (per launch averages over the timed steps)
+    class S:  # aggregate stats as an object for algorithmic_bytes
+        dedup_probes = sum(x[2] for x in stats)
+        dedup_inserts = sum(x[3] for x in stats)
+        donations = sum(x[4] for x in stats)
+    launches = sum(x[5] for x in stats)
+    bytes_total = algorithmic_bytes(S, args.batch * args.steps)
+    peak, peak_kind = measured_hbm()
+    achieved = bytes_total / device_s / 1e9
+    line = {
+        "metric": "cases resolved/s (config-2 3-permutations, full sorting, ratio 1.375, depth 11)",
+        "value": round(value, 3),
+        "unit": "cases/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(device_s * 1e3 / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic (seeded 3-permutations, numpy PCG64)",
+        "config": {"workload": ("config2: 100,000 seeded 3-permutations, m~U{4..8} (n<=24)" if config_id == 2 else
+                                 "config1: seeded 3-permutations, m~U{4,5,6} (n<=18)") +
+                                ", full sorting, ratio 1.375, max depth 11, 3000 MB queue budget, 1 slot",
+                   "table_entries": args.table_entries, "batch_per_step": args.batch, "l2": "flushed by a 256 MB write between steps",
+                   "parallelism": f"replicas x{world} (cases sharded, no collective)"},
+        "nodes_per_s": round(nodes / (sum(kernel_ms) / 1e3), 1),
+        "verdicts": {"found": found, "not_found": notfound, "other": other},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 3), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 6), "traffic": None,
+                     "note": f"algorithmic table/task/instance bytes over kernel time; peak {peak_kind}"},
+        "e2e": {"value": round(cases / wall, 3) if wall > 0 else None, "unit": "cases/s",
+                "h2d_bytes_per_step": args.batch * 144, "d2h_bytes_per_step": args.batch * 96},
+        "clocks": clocks.summary(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = {"value": round(cpu[0], 4), "unit": "cases/s", "cores": cpu[2], "kind": "port",
+                                "sample": cpu[3], "nodes_per_s": round(cpu[1], 1)}
+    GPUSortingSearch.destroySlots()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    samples = []
+    first = 0
+    for s in range(args.warmup + args.steps):
+        cps, nps, cores, detail = cpu_sample(args.cpu_budget_s, args.cpu_node_limit, first_case=first)
+        first += 4 * cores
+        if s >= args.warmup:
+            samples.append((cps, nps))
+    value = sum(x[0] for x in samples) / len(samples)
+    line = {
+        "impl": "reference",
+        "metric": "cases resolved/s (config-2 3-permutations, full sorting, ratio 1.375, depth 11)",
+        "value": round(value, 4),
+        "unit": "cases/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(args.cpu_budget_s * 1e3, 1),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic (seeded 3-permutations, numpy PCG64)",
+        "config": {"workload": "config2: 100,000 seeded 3-permutations, m~U{4..8} (n<=24), full sorting, "
+                               "ratio 1.375, max depth 11", "parallelism": "host cores"},
+        "nodes_per_s": round(sum(x[1] for x in samples) / len(samples), 1),
+        "cpu_baseline": {"value": round(value, 4), "unit": "cases/s", "cores": cores, "kind": "port",
+                         "sample": detail},
+        "e2e": {"value": round(value, 4), "unit": "cases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -198,13 +198,6 @@ struct LaneStats {
     unsigned long long probes = 0, pruned = 0, inserts = 0, full = 0;
 };
 
-__device__ __forceinline__ bool tag_reclaimable(const EngineParams &P, uint32_t t) {
-    if (t == 0u) return true;
-    if ((t >> kInstanceBits) != P.generation) return true;
-    const uint32_t idx = t & ((1u << kInstanceBits) - 1u);
-    return (ld_relaxed_u32(P.doneBits + (idx >> 5)) >> (idx & 31u)) & 1u;
-}
-
 // Transposition-table admission (sorting_search.cu:261-298 semantics, per instance).
 template <int KW>
 __device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t tag, const uint64_t (&key)[KW],
@@ -215,8 +208,7 @@ __device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t tag,
     uint32_t tags[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) tags[q] = ld_acquire_u32(&table[base + q].tag);
-    int freeSlot = -1;
-    uint32_t freeTag = 0;
+    unsigned freeMask = 0;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         const uint32_t t = tags[q];
@@ -233,11 +225,27 @@ __device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t tag,
                 }
                 return true;
             }
-        } else if (freeSlot < 0 && t != kTagWriting && tag_reclaimable(P, t)) {
-            freeSlot = q;
-            freeTag = t;
+        } else if (t == 0u || (t != kTagWriting && (t >> kInstanceBits) != P.generation)) {
+            freeMask |= 1u << q;
         }
     }
+    if (freeMask == 0u) {
+        // No empty or old-generation slot: look for entries of finished instances, with
+        // the eight done-bit loads issued together.
+        uint32_t done[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t idx = tags[q] & ((1u << kInstanceBits) - 1u);
+            done[q] = (tags[q] != kTagWriting) ? ld_relaxed_u32(P.doneBits + (idx >> 5)) : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t idx = tags[q] & ((1u << kInstanceBits) - 1u);
+            if (tags[q] != kTagWriting && ((done[q] >> (idx & 31u)) & 1u)) freeMask |= 1u << q;
+        }
+    }
+    const int freeSlot = freeMask ? (__ffs(freeMask) - 1) : -1;
+    const uint32_t freeTag = freeSlot >= 0 ? tags[freeSlot] : 0u;
     if (freeSlot >= 0) {
         DedupEntry<KW> *e = &table[base + freeSlot];
         if (atomicCAS(&e->tag, freeTag, kTagWriting) == freeTag) {
@@ -443,17 +451,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
                     poll = 0;
                     int act = 0;
                     if (lane == 0) {
-                        if (ld_relaxed_s32(&ctl->stop) || ld_relaxed_s32(P.cancel)) {
+                        // Independent loads, issued together: one L2 round trip per poll.
+                        const int stopFlag = ld_relaxed_s32(&ctl->stop);
+                        const int cancelFlag = ld_relaxed_s32(P.cancel);
+                        const int state = ld_relaxed_s32(&P.out[inst].state);
+                        const int hg = ld_relaxed_s32(&ctl->hungry);
+                        const int top = ld_relaxed_s32(&ctl->taskTop);
+                        const bool late = global_time_ns() > deadline;
+                        if (stopFlag | cancelFlag) {
                             act = 2;
-                        } else if (global_time_ns() > deadline) {
+                        } else if (late) {
                             atomicExch(&ctl->error, kErrDeadline);
                             atomicExch(&ctl->stop, 1);
                             act = 2;
-                        } else if (ld_relaxed_s32(&P.out[inst].state) == kStateFound) {
+                        } else if (state == kStateFound) {
                             act = 1;
-                        } else {
-                            const int hg = ld_relaxed_s32(&ctl->hungry);
-                            if (hg > 0 && ld_relaxed_s32(&ctl->taskTop) < hg) act = 3;
+                        } else if (hg > 0 && top < hg) {
+                            act = 3;
                         }
                     }
                     act = __shfl_sync(kFull, act, 0);

@@ -88,7 +88,7 @@ def _small_cases():
     return out
 
 
-@pytest.mark.parametrize("full,depth", [(True, 5), (False, 4), (True, 7)])
+@pytest.mark.parametrize("full,depth", [(True, 5), (False, 4), (True, 6)])
 def test_transposition_table_and_tight_bound_keep_verdicts(oracle, full, depth):
     """The oracle with the transposition table, and with the tight bound, answers like
     the plain exhaustive restatement (no table, no tight bound)."""
@@ -101,10 +101,10 @@ def test_transposition_table_and_tight_bound_keep_verdicts(oracle, full, depth):
 
 def test_java_rule_and_cuda_rule_agree_on_small_full_sorting(oracle):
     """SortingSearch.java's double-precision rule and the CUDA float rule give the same
-    verdicts away from the k = 11 hazard (here max depth 7)."""
+    verdicts away from the k = 11 hazard (here max depth 6)."""
     for pi, spi, even in _small_cases():
-        g = oracle.search_gpu_rule(list(pi), list(spi), even, R1375, 7, True)[0]
-        c, syms, _ = oracle.search_cpu_rule(list(pi), list(spi), even, R1375, 7, node_limit=2_000_000)
+        g = oracle.search_gpu_rule(list(pi), list(spi), even, R1375, 6, True)[0]
+        c, syms, _ = oracle.search_cpu_rule(list(pi), list(spi), even, R1375, 6, node_limit=2_000_000)
         assert c == g
         if c == 1:
             e, final = oracle.replay_symbols(list(pi), list(spi), syms)

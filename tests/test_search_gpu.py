@@ -61,9 +61,9 @@ def test_config1_verdicts_match_oracle(gpu_searcher, oracle):
     rows = data["cases"]
     n = max(r["case"] for r in rows) + 1
     cases = list(config_cases(1, n))
-    for key, full, depth in (("full11", True, 11), ("partial6", False, 6)):
+    for key, full, depth in (("full11", True, 11), ("full7", True, 7), ("partial6", False, 6)):
         sel = [r for r in rows if r[key] in (0, 1)]
-        assert len(sel) > 50
+        assert len(sel) > 50, key
         batch = [cases[r["case"]][:3] for r in sel]
         res = run_batch(batch, depth, full, R1375)
         for row, case, r in zip(sel, batch, res):
