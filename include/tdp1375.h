@@ -121,6 +121,8 @@ typedef struct tdp_engine_config {
     int32_t tight_bound;     /* 1 = verdict-preserving strengthened prune, 0 = reference prune only */
     int32_t task_capacity;   /* donation pool entries (<= queue budget) */
     double time_limit_s;     /* device deadline per launch */
+    int32_t sparse_enumeration; /* 1 = same-cycle pair enumeration where -2 children are useless */
+    int32_t reserved;
 } tdp_engine_config;
 
 int tdp_get_engine_config(int slot, tdp_engine_config *cfg);

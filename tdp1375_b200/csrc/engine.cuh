@@ -68,17 +68,21 @@ enum EngineStat : int {
     kStatCount
 };
 
-// Launch-wide control block, zeroed before every launch.
-struct EngineCtl {
-    int nextInstance;
-    int doneCount;
-    int hungry;
-    int taskTop;
+// Launch-wide control block, zeroed before every launch.  Fields that thousands of warps
+// poll live on separate 128-byte lines so one hot line does not serialise the others.
+struct alignas(128) EngineCtl {
+    int taskTop;  // line 0: donation pool
     int taskLock;
-    int stop;
+    int pad0[30];
+    int hungry;  // line 1: idle warps
+    int pad1[31];
+    int nextInstance;  // line 2: instance admission / completion
+    int doneCount;
+    int pad2[30];
+    int stop;  // line 3: launch stop + error
     int error;
-    int reserved;
-    unsigned long long stats[kStatCount];
+    int pad3[30];
+    unsigned long long stats[kStatCount];  // line 4
 };
 
 enum EngineError : int {
@@ -116,6 +120,7 @@ struct EngineParams {
     EngineCtl *ctl;
     const int *cancel;        // slot cancel flag (device)
     unsigned long long timeLimitNs;  // every warp stops (error kErrDeadline) after this long
+    int sparse;                      // same-cycle pair enumeration allowed (n <= 32)
 };
 
 }  // namespace tdp

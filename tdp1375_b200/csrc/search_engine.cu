@@ -271,6 +271,7 @@ void SearchSlot::launchClass(int cls, int offset, int count) {
     P.ctl = dCtl_;
     P.cancel = dCancel_;
     P.timeLimitNs = (unsigned long long)(std::max(0.001, cfg_.time_limit_s) * 1e9);
+    P.sparse = cfg_.sparse_enumeration;
 
     int blocksPerSM = 0;
     const int threads = dev::kWarpsPerBlock * 32;

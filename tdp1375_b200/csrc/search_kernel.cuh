@@ -195,7 +195,7 @@ __device__ __forceinline__ uint64_t key_hash(const uint64_t (&k)[KW], uint32_t t
 }
 
 struct LaneStats {
-    unsigned long long probes = 0, pruned = 0, inserts = 0, full = 0;
+    unsigned probes = 0, pruned = 0, inserts = 0, full = 0;
 };
 
 // Transposition-table admission (sorting_search.cu:261-298 semantics, per instance).
@@ -280,14 +280,89 @@ __device__ __forceinline__ void lock_release(EngineCtl *ctl) {
     atomicExch(&ctl->taskLock, 0);
 }
 
+// Same-cycle pair enumeration.  When a frame's children can neither succeed nor be
+// admitted with a -2 change, and either 0-changes are useless too or the node has at most
+// one even-length cycle, every child worth evaluating has two of its three symbols in one
+// spi-cycle (a triple over three distinct cycles changes the odd-cycle count by -2, or by 0
+// only when two of the cycles have even length).  Such a frame enumerates pairs of
+// positions p < q whose symbols share a cycle, one pair per chunk, with the lane as the
+// third position r; a triple lying in one cycle is taken only from its two smallest
+// positions.  Only for n <= 32 (one position per lane).
+struct SparseFrame {
+    uint32_t same;       // positions > lane whose symbol shares the cycle of pi[lane]
+    uint32_t incl;       // inclusive prefix of popc(same) over lanes
+    uint32_t leaderPos;  // cycle leader of pi[lane]
+    int np;              // number of pairs
+    bool on;
+};
+
+struct PairSel {
+    int p, q;
+    uint32_t leader;
+};
+
+template <int NW>
+__device__ __forceinline__ SparseFrame sparse_setup(const uint32_t (&w)[NW], int n, int lane, int even,
+                                                    uint64_t satMask, uint64_t expMask, int enable) {
+    SparseFrame sf;
+    sf.same = 0u;
+    sf.incl = 0u;
+    sf.leaderPos = 0u;
+    sf.np = 0;
+    sf.on = false;
+    if constexpr (NW != 1) {
+        return sf;
+    } else {
+        if (!enable) return sf;
+        const uint64_t useful = satMask | expMask;
+        const bool neg = even >= 2 && ((useful >> (even - 2)) & 1ull);
+        if (neg) return sf;
+        const bool zero = (useful >> even) & 1ull;
+        const bool isLeader = lane < n && w_leader(w[0]) == (uint32_t)lane;
+        const int evenLen = __popc(__ballot_sync(kFull, isLeader && (w_len(w[0]) & 1u) == 0u));
+        if (zero && evenLen >= 2) return sf;
+        const uint32_t leaderPos = w_leader(gather<1>(w, w_pi(w[0])));
+        const uint32_t key = (lane < n) ? leaderPos : 64u + (uint32_t)lane;
+        const uint32_t same = __match_any_sync(kFull, key) & ~((2u << lane) - 1u);
+        uint32_t incl = (uint32_t)__popc(same);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        sf.same = same;
+        sf.incl = incl;
+        sf.leaderPos = leaderPos;
+        sf.np = (int)__shfl_sync(kFull, incl, 31);
+        sf.on = true;
+        return sf;
+    }
+}
+
+// Decodes pair index u (uniform) into positions p < q.
+__device__ __forceinline__ PairSel sparse_pair(const SparseFrame &sf, int u) {
+    const unsigned owner = __ballot_sync(kFull, sf.incl > (uint32_t)u);
+    const int p = __ffs(owner) - 1;
+    const uint32_t sameP = __shfl_sync(kFull, sf.same, p);
+    const uint32_t exclP = __shfl_sync(kFull, sf.incl, p) - (uint32_t)__popc(sameP);
+    uint32_t m = sameP;
+    for (uint32_t t = (uint32_t)u - exclP; t > 0u; --t) m &= m - 1u;
+    PairSel ps;
+    ps.p = p;
+    ps.q = __ffs(m) - 1;
+    ps.leader = __shfl_sync(kFull, sf.leaderPos, p);
+    return ps;
+}
+
 template <int NW>
 struct WarpShared {
     uint32_t words[kMaxDepth + 1][NW * 32];
     uint32_t staging[52];
+    unsigned long long stats[kStatCount];  // per-warp counters, flushed once at exit
 };
 
 template <int NW>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(const EngineParams P) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_engine_kernel(const EngineParams P) {
     using K = KeyTraits<NW>;
     constexpr int KW = K::KW;
     __shared__ WarpShared<NW> smem[kWarpsPerBlock];
@@ -296,21 +371,33 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
     EngineCtl *ctl = P.ctl;
     const unsigned long long deadline = global_time_ns() + P.timeLimitNs;
 
-    unsigned long long wNodes = 0, wChildren = 0, wDonations = 0, wPops = 0;
+    if (lane < kStatCount) S.stats[lane] = 0ull;
+    __syncwarp();
     LaneStats ls;
     bool hungry = false;
-    int backoff = 32;
+    int backoff = 256;
+    int idleRound = 0;
     bool stopAll = false;
 
     while (!stopAll) {
         // ---------------------------------------------------------------- get work
         int kind = 0, idx = 0;
         if (lane == 0) {
-            if (ld_relaxed_s32(&ctl->stop) || ld_relaxed_s32(P.cancel) || global_time_ns() > deadline) {
-                if (global_time_ns() > deadline) {
+            // Idle warps read only the donation line every round; the admission, completion
+            // and stop lines every 8th round (busy warps poll stop/cancel themselves).
+            const bool full = hungry ? ((++idleRound & 7) == 0) : true;
+            bool quit = false;
+            if (full) {
+                const int stopFlag = ld_relaxed_s32(&ctl->stop);
+                const int cancelFlag = ld_relaxed_s32(P.cancel);
+                const bool late = global_time_ns() > deadline;
+                if (late && !(stopFlag | cancelFlag)) {
                     atomicExch(&ctl->error, kErrDeadline);
                     atomicExch(&ctl->stop, 1);
                 }
+                quit = (stopFlag | cancelFlag) || late;
+            }
+            if (quit) {
                 kind = -1;
             } else {
                 if (ld_relaxed_s32(&ctl->taskTop) > 0) {
@@ -328,14 +415,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
                         kind = -1;
                     }
                 }
-                if (kind == 0 && ld_relaxed_s32(&ctl->nextInstance) < P.count) {
+                if (kind == 0 && full && ld_relaxed_s32(&ctl->nextInstance) < P.count) {
                     const int i = atomicAdd(&ctl->nextInstance, 1);
                     if (i < P.count) {
                         kind = 2;
                         idx = i;
                     }
                 }
-                if (kind == 0 && ld_relaxed_s32(&ctl->doneCount) >= P.count) kind = -1;
+                if (kind == 0 && full && ld_relaxed_s32(&ctl->doneCount) >= P.count) kind = -1;
             }
         }
         kind = __shfl_sync(kFull, kind, 0);
@@ -345,12 +432,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
             if (!hungry && lane == 0) atomicAdd(&ctl->hungry, 1);
             hungry = true;
             __nanosleep(backoff);
-            backoff = min(backoff * 2, 4096);
+            backoff = min(backoff * 2, 32768);
             continue;
         }
         if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
         hungry = false;
-        backoff = 32;
+        backoff = 256;
+        idleRound = 0;
 
         // ---------------------------------------------------------------- set up
         uint32_t inst;
@@ -363,7 +451,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
             for (int q = lane; q < 52; q += 32) S.staging[q] = __ldcg(src + q);
             __syncwarp();
             if (lane == 0) lock_release(ctl);
-            ++wPops;
+            if (lane == 0) ++S.stats[kStatTaskPops];
             inst = S.staging[0];
             baseDepth = (int)(S.staging[1] & 0xFFu);
             even = (int)((S.staging[1] >> 8) & 0xFFu);
@@ -411,7 +499,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
         int f = baseDepth;
         int cursor = lo, end = hi, chunk = 0;
         uint32_t pending = 0;
-        int fCursor = 0, fEnd = 0, fChunk = 0, fEven = 0;
+        int fCursor = 0, fEnd = 0, fChunk = 0, fEven = 0, fStep = 32;
         uint32_t fPending = 0;
         uint64_t fKey[KW];
 #pragma unroll
@@ -420,6 +508,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
         for (int h = 0; h < NW; ++h) S.words[f][h * 32 + lane] = w[h];
         uint64_t satMask = shfl64(ruleReg, f + 1);
         uint64_t expMask = shfl64(ruleReg, 16 + f + 1);
+        SparseFrame sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse);
+        // A donated range is in the units of its frame's mode (the receiver derives the same
+        // mode from the same node); a root covers every child.
+        if (kind == 2) end = sf.on ? sf.np : T;
 
         // outcome: 0 subtree exhausted, 1 instance found (here or elsewhere), 2 launch stop
         int outcome = 0;
@@ -445,6 +537,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
                     for (int h = 0; h < NW; ++h) w[h] = S.words[f][h * 32 + lane];
                     satMask = shfl64(ruleReg, f + 1);
                     expMask = shfl64(ruleReg, 16 + f + 1);
+                    sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse);
                     continue;
                 }
                 if (++poll >= P.pollInterval) {
@@ -477,19 +570,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
                     }
                     if (act == 3) {
                         // ------------------------------------------------ donate
-                        int rem = 0;
-                        if (lane >= baseDepth && lane < f) rem = fEnd - fCursor;
-                        if (lane == f) rem = end - cursor;
-                        const unsigned big = __ballot_sync(kFull, rem >= 64);
-                        const unsigned some = __ballot_sync(kFull, rem > 0 && lane < f);
+                        const int step = sf.on ? 1 : 32;
+                        int remChunks = 0;
+                        if (lane >= baseDepth && lane < f) remChunks = (fEnd - fCursor + fStep - 1) / fStep;
+                        if (lane == f) remChunks = (end - cursor + step - 1) / step;
+                        const unsigned big = __ballot_sync(kFull, remChunks >= 2);
+                        const unsigned some = __ballot_sync(kFull, remChunks > 0 && lane < f);
                         const int g = big ? (__ffs(big) - 1) : (some ? (__ffs(some) - 1) : -1);
                         if (g >= 0) {
                             const int gc = __shfl_sync(kFull, (lane == f) ? cursor : fCursor, g);
                             const int ge = __shfl_sync(kFull, (lane == f) ? end : fEnd, g);
                             const int gEven = __shfl_sync(kFull, (lane == f) ? even : fEven, g);
-                            const int remg = ge - gc;
-                            const int keepChunks = (remg >= 64) ? (((remg + 31) / 32 + 1) / 2) : 0;
-                            const int newEnd = min(ge, gc + keepChunks * 32);
+                            const int gStep = __shfl_sync(kFull, (lane == f) ? step : fStep, g);
+                            const int remg = (ge - gc + gStep - 1) / gStep;
+                            const int keepChunks = (remg >= 2) ? (remg + 1) / 2 : 0;
+                            const int newEnd = min(ge, gc + keepChunks * gStep);
                             int slot = -1;
                             if (lane == 0 && newEnd < ge) {
                                 atomicAdd(&P.out[inst].outstanding, 1);
@@ -535,7 +630,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
                                 } else if (lane == g) {
                                     fEnd = newEnd;
                                 }
-                                ++wDonations;
+                                if (lane == 0) ++S.stats[kStatDonations];
                             }
                         }
                         // The donor keeps at least one chunk of its current frame
@@ -543,20 +638,48 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
                     }
                 }
                 // ---------------------------------------------------- evaluate a chunk
+                uint32_t tr, a, b, c;
+                bool valid;
+                int nValid;
                 chunk = cursor;
-                const int t = cursor + lane;
-                cursor += 32;
-                const bool valid = t < end;
-                const uint32_t tr = valid ? __ldg(trip + t) : 0u;
-                const uint32_t a = w_pi(gather<NW>(w, tri_i(tr)));
-                const uint32_t b = w_pi(gather<NW>(w, tri_j(tr)));
-                const uint32_t c = w_pi(gather<NW>(w, tri_k(tr)));
+                if (sf.on) {
+                    // one same-cycle position pair (p, q) per chunk, lane = third position r
+                    cursor += 1;
+                    const PairSel ps = sparse_pair(sf, chunk);
+                    const uint32_t r = (uint32_t)lane;
+                    valid = (int)r < n && (int)r != ps.p && (int)r != ps.q &&
+                            (sf.leaderPos != ps.leader || (int)r > ps.q);
+                    const uint32_t symP = w_pi(__shfl_sync(kFull, w[0], ps.p));
+                    const uint32_t symQ = w_pi(__shfl_sync(kFull, w[0], ps.q));
+                    const uint32_t symR = w_pi(w[0]);
+                    if ((int)r < ps.p) {
+                        tr = pack_triple(r, ps.p, ps.q);
+                        a = symR, b = symP, c = symQ;
+                    } else if ((int)r < ps.q) {
+                        tr = pack_triple(ps.p, r, ps.q);
+                        a = symP, b = symR, c = symQ;
+                    } else {
+                        tr = pack_triple(ps.p, ps.q, r);
+                        a = symP, b = symQ, c = symR;
+                    }
+                    if (!valid) tr = a = b = c = 0u;
+                    nValid = __popc(__ballot_sync(kFull, valid));
+                } else {
+                    const int t = cursor + lane;
+                    cursor += 32;
+                    valid = t < end;
+                    tr = valid ? __ldg(trip + t) : 0u;
+                    a = w_pi(gather<NW>(w, tri_i(tr)));
+                    b = w_pi(gather<NW>(w, tri_j(tr)));
+                    c = w_pi(gather<NW>(w, tri_k(tr)));
+                    nValid = min(32, end - chunk);
+                }
                 const uint32_t wa = gather<NW>(w, a);
                 const uint32_t wb = gather<NW>(w, b);
                 const uint32_t wc = gather<NW>(w, c);
                 const int e = even + move_delta(wa, wb, wc);
                 const bool sat = valid && ((satMask >> e) & 1ull);
-                tChildren += (unsigned long long)min(32, end - chunk);
+                tChildren += (unsigned long long)nValid;
                 const unsigned satBallot = __ballot_sync(kFull, sat);
                 if (satBallot) {
                     const int winner = __ffs(satBallot) - 1;
@@ -591,13 +714,22 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
             // -------------------------------------------------------- descend
             const int l = __ffs(pending) - 1;
             pending &= pending - 1u;
-            const uint32_t tr = __ldg(trip + chunk + l);
+            uint32_t tr;
+            if (sf.on) {
+                const PairSel ps = sparse_pair(sf, chunk);
+                const int r = l;
+                tr = (r < ps.p) ? pack_triple(r, ps.p, ps.q)
+                                : (r < ps.q) ? pack_triple(ps.p, r, ps.q) : pack_triple(ps.p, ps.q, r);
+            } else {
+                tr = __ldg(trip + chunk + l);
+            }
             if (lane == f) {
                 fCursor = cursor;
                 fEnd = end;
                 fPending = pending;
                 fChunk = chunk;
                 fEven = even;
+                fStep = sf.on ? 1 : 32;
                 fMove = tr;
 #pragma unroll
                 for (int q = 0; q < KW; ++q) fKey[q] = key[q];
@@ -630,15 +762,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
             ++f;
 #pragma unroll
             for (int h = 0; h < NW; ++h) S.words[f][h * 32 + lane] = w[h];
-            cursor = 0;
-            end = T;
-            pending = 0u;
             satMask = shfl64(ruleReg, f + 1);
             expMask = shfl64(ruleReg, 16 + f + 1);
+            sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse);
+            cursor = 0;
+            end = sf.on ? sf.np : T;
+            pending = 0u;
             ++tNodes;
         }
-        wNodes += tNodes;
-        wChildren += tChildren;
+        if (lane == 0) {
+            S.stats[kStatNodes] += tNodes;
+            S.stats[kStatChildren] += tChildren;
+        }
         if (outcome == 2) {
             stopAll = true;
             break;
@@ -660,7 +795,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
     if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
 
     // ---------------------------------------------------------------- statistics
-    unsigned long long probes = ls.probes, pruned = ls.pruned, inserts = ls.inserts, full = ls.full;
+    unsigned long long probes = ls.probes, pruned = ls.pruned, inserts = ls.inserts, full = ls.full;  // widen once
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         probes += __shfl_xor_sync(kFull, probes, o);
@@ -669,14 +804,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_engine_kernel(cons
         full += __shfl_xor_sync(kFull, full, o);
     }
     if (lane == 0) {
-        atomicAdd(&ctl->stats[kStatNodes], wNodes);
-        atomicAdd(&ctl->stats[kStatChildren], wChildren);
+        atomicAdd(&ctl->stats[kStatNodes], S.stats[kStatNodes]);
+        atomicAdd(&ctl->stats[kStatChildren], S.stats[kStatChildren]);
         atomicAdd(&ctl->stats[kStatDedupProbes], probes);
         atomicAdd(&ctl->stats[kStatDedupPruned], pruned);
         atomicAdd(&ctl->stats[kStatDedupInserts], inserts);
         atomicAdd(&ctl->stats[kStatDedupFull], full);
-        atomicAdd(&ctl->stats[kStatDonations], wDonations);
-        atomicAdd(&ctl->stats[kStatTaskPops], wPops);
+        atomicAdd(&ctl->stats[kStatDonations], S.stats[kStatDonations]);
+        atomicAdd(&ctl->stats[kStatTaskPops], S.stats[kStatTaskPops]);
     }
 }
 

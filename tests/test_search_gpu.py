@@ -73,23 +73,30 @@ def test_config1_verdicts_match_oracle(gpu_searcher, oracle):
                 assert ok
 
 
-def test_single_and_batch_agree_and_tight_bound_keeps_verdicts(gpu_searcher, oracle):
+@pytest.mark.parametrize("full,depth", [(False, 8), (True, 11)])
+def test_engine_modes_keep_verdicts(gpu_searcher, oracle, full, depth):
+    """Single-instance calls, batched calls, and the engine with the tight bound and/or
+    the same-cycle pair enumeration switched off all give the same verdicts."""
     from tdp1375_b200 import GPUSortingSearch, api, native
     from tdp1375_b200.cases import config_cases
-    cases = [c[:3] for c in config_cases(2, 40)]
-    batch = run_batch(cases, 8, False, R1375)
+    cases = [c[:3] for c in config_cases(1, 40)]
+    batch = run_batch(cases, depth, full, R1375)
     cfg = api.engine_config(1)
-    loose = native.EngineConfig(cfg.blocks_per_sm, cfg.poll_interval, 0, cfg.task_capacity, cfg.time_limit_s)
-    api.set_engine_config(1, loose)
-    try:
-        ref_prune = run_batch(cases, 8, False, R1375, slot=1)
-    finally:
-        api.set_engine_config(1, cfg)
-    for (pi, spi, even), b, c in zip(cases, batch, ref_prune):
-        pos = GPUSortingSearch.searchForSortingSeq(list(pi), list(spi), even, R1375, 8, False, 0)
-        assert (1 if pos else 0) == b.status == c.status
-        if pos:
-            ok, _ = oracle.replay_positions(list(pi), list(spi), pos, even, R1375, False)
+    variants = []
+    for tight, sparse in ((1, 0), (0, 0), (0, 1)):
+        api.set_engine_config(1, native.EngineConfig(cfg.blocks_per_sm, cfg.poll_interval, tight, cfg.task_capacity,
+                                                     cfg.time_limit_s, sparse, 0))
+        try:
+            variants.append(run_batch(cases, depth, full, R1375, slot=1))
+        finally:
+            api.set_engine_config(1, cfg)
+    for idx, ((pi, spi, even), b) in enumerate(zip(cases, batch)):
+        assert all(v[idx].status == b.status for v in variants), idx
+        if idx < 10:
+            pos = GPUSortingSearch.searchForSortingSeq(list(pi), list(spi), even, R1375, depth, full, 0)
+            assert (1 if pos else 0) == b.status
+        if b.status == 1:
+            ok, _ = oracle.replay_positions(list(pi), list(spi), positions(b), even, R1375, full)
             assert ok
 
 
