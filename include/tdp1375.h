@@ -130,6 +130,42 @@ int tdp_set_engine_config(int slot, const tdp_engine_config *cfg);
 
 int tdp_device_count(void);
 
+/* ---- learned move ordering (no counterpart in the reference) ------------------------
+ * A 1088 -> 256 -> 256 -> 256 -> 5456 BF16 MLP (fp32 accumulation on the tcgen05 tensor
+ * cores) scores the (i,j,k) triples of a configuration with n <= 32; the batched search then
+ * expands each instance's root children in descending score order.  Ordering only permutes
+ * children: verdicts are unchanged.  The entry points below take DEVICE pointers and a
+ * cudaStream_t (as void*); they are the building blocks of inference and training. */
+#define TDP_MLP_FEATURES 1088
+#define TDP_MLP_HIDDEN 256
+#define TDP_MLP_TRIPLES 5456
+#define TDP_MLP_TRIPLES_PADDED 5632
+
+/* C[m x n] = A[m x k] * B[n x k]^T (+bias[n]) (ReLU if relu); A, B bf16 row-major, k % 8 == 0,
+ * 16-byte aligned; out bf16 (out_fp32 = 0) or fp32 with row stride ldo. */
+int tdp_mlp_gemm(const void *a, const void *b, int m, int n, int k, const float *bias, int relu, void *out,
+                 int out_fp32, int ldo, void *stream);
+/* Features of count states (spi/pi rows of 64 bytes, n[count]) into x [count x 1088] bf16. */
+int tdp_mlp_features(const uint8_t *spi, const uint8_t *pi, const uint8_t *n, int count, void *x, void *stream);
+int tdp_mlp_softmax_xent(const float *logits, int ld, const uint8_t *n, const int32_t *target, int rows,
+                         void *dlogits, float *loss, void *stream);
+int tdp_mlp_transpose(const void *in, int rows, int cols, void *out, void *stream);
+int tdp_mlp_relu_backward(void *grad, const void *act, int64_t count, void *stream);
+int tdp_mlp_column_sums(const void *grad, int rows, int cols, float *out, void *stream);
+int tdp_mlp_adam(float *master, void *weight, const float *grad, float *m, float *v, int64_t count, float lr,
+                 float beta1, float beta2, float eps, int step, void *stream);
+int tdp_mlp_order(const float *scores, int ld, const uint8_t *n, int count, uint16_t *order, int order_stride,
+                  void *stream);
+/* 0 when no tensor-core wait has timed out since the last call (the flag is then cleared). */
+int tdp_mlp_error(void);
+
+/* Installs the ordering model on a slot (host arrays: bf16 weights as uint16 bits in the
+ * torch.nn.Linear [out, in] layout, fp32 biases; w4 has 5456 rows).  enable = 0 keeps the
+ * weights but searches in plain order. */
+int tdp_set_order_model(int slot, const uint16_t *w1, const float *b1, const uint16_t *w2, const float *b2,
+                        const uint16_t *w3, const float *b3, const uint16_t *w4, const float *b4);
+int tdp_enable_order_model(int slot, int enable);
+
 #ifdef __cplusplus
 }
 #endif

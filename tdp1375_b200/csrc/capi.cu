@@ -230,3 +230,122 @@ int64_t tdp_pi_filter(const uint8_t *cycle, int cycle_len, const uint8_t *orient
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- move-ordering MLP
+#include "mlp.h"
+
+namespace {
+
+int *mlp_error_flag() {
+    static std::mutex mu;
+    static std::vector<int *> flags;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)flags.size() <= dev) flags.resize(dev + 1, nullptr);
+    if (!flags[dev]) {
+        int *p = nullptr;
+        if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
+        cudaMemset(p, 0, sizeof(int));
+        flags[dev] = p;
+    }
+    return flags[dev];
+}
+
+int launch_status(const char *what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(TDP_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tdp_mlp_gemm(const void *a, const void *b, int m, int n, int k, const float *bias, int relu, void *out,
+                 int out_fp32, int ldo, void *stream) {
+    int *flag = mlp_error_flag();
+    if (!flag) return fail(TDP_ERR_OUT_OF_MEMORY, "tdp_mlp_gemm: error flag allocation failed");
+    std::string err;
+    const int rc = tdp::mlp::gemm_bf16(a, b, m, n, k, bias, relu, out, out_fp32, ldo, flag,
+                                       static_cast<cudaStream_t>(stream), err);
+    if (rc != 0) return fail(rc == -1 ? TDP_ERR_ARGUMENT : TDP_ERR_CUDA, err);
+    return 0;
+}
+
+int tdp_mlp_error(void) {
+    int *flag = mlp_error_flag();
+    if (!flag) return fail(TDP_ERR_OUT_OF_MEMORY, "tdp_mlp_error: error flag allocation failed");
+    int host = 0;
+    if (cudaMemcpy(&host, flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(TDP_ERR_CUDA, "tdp_mlp_error: read failed");
+    if (host) cudaMemset(flag, 0, sizeof(int));
+    return host;
+}
+
+int tdp_mlp_features(const uint8_t *spi, const uint8_t *pi, const uint8_t *n, int count, void *x, void *stream) {
+    tdp::mlp::build_features(spi, pi, n, 64, 1, count, static_cast<__nv_bfloat16 *>(x), static_cast<cudaStream_t>(stream));
+    return launch_status("tdp_mlp_features");
+}
+
+int tdp_mlp_softmax_xent(const float *logits, int ld, const uint8_t *n, const int32_t *target, int rows,
+                         void *dlogits, float *loss, void *stream) {
+    tdp::mlp::softmax_xent(logits, ld, n, target, rows, static_cast<__nv_bfloat16 *>(dlogits), loss,
+                           static_cast<cudaStream_t>(stream));
+    return launch_status("tdp_mlp_softmax_xent");
+}
+
+int tdp_mlp_transpose(const void *in, int rows, int cols, void *out, void *stream) {
+    tdp::mlp::transpose_bf16(static_cast<const __nv_bfloat16 *>(in), rows, cols, static_cast<__nv_bfloat16 *>(out),
+                             static_cast<cudaStream_t>(stream));
+    return launch_status("tdp_mlp_transpose");
+}
+
+int tdp_mlp_relu_backward(void *grad, const void *act, int64_t count, void *stream) {
+    tdp::mlp::relu_backward(static_cast<__nv_bfloat16 *>(grad), static_cast<const __nv_bfloat16 *>(act),
+                            (size_t)count, static_cast<cudaStream_t>(stream));
+    return launch_status("tdp_mlp_relu_backward");
+}
+
+int tdp_mlp_column_sums(const void *grad, int rows, int cols, float *out, void *stream) {
+    tdp::mlp::column_sums(static_cast<const __nv_bfloat16 *>(grad), rows, cols, out, static_cast<cudaStream_t>(stream));
+    return launch_status("tdp_mlp_column_sums");
+}
+
+int tdp_mlp_adam(float *master, void *weight, const float *grad, float *m, float *v, int64_t count, float lr,
+                 float beta1, float beta2, float eps, int step, void *stream) {
+    tdp::mlp::adam_step(master, static_cast<__nv_bfloat16 *>(weight), grad, m, v, (size_t)count, lr, beta1, beta2,
+                        eps, step, static_cast<cudaStream_t>(stream));
+    return launch_status("tdp_mlp_adam");
+}
+
+int tdp_mlp_order(const float *scores, int ld, const uint8_t *n, int count, uint16_t *order, int order_stride,
+                  void *stream) {
+    tdp::mlp::order_by_score(scores, ld, n, 1, count, order, order_stride, static_cast<cudaStream_t>(stream));
+    return launch_status("tdp_mlp_order");
+}
+
+int tdp_set_order_model(int slot, const uint16_t *w1, const float *b1, const uint16_t *w2, const float *b2,
+                        const uint16_t *w3, const float *b3, const uint16_t *w4, const float *b4) {
+    auto s = get_slot(slot);
+    if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    if (!w1 || !b1 || !w2 || !b2 || !w3 || !b3 || !w4 || !b4) return fail(TDP_ERR_ARGUMENT, "tdp_set_order_model: null array");
+    try {
+        std::string err;
+        const int rc = s->setOrderModel(w1, b1, w2, b2, w3, b3, w4, b4, err);
+        if (rc != 0) return fail(rc, err);
+        return 0;
+    } catch (const std::exception &e) {
+        return map_exception(e);
+    }
+}
+
+int tdp_enable_order_model(int slot, int enable) {
+    auto s = get_slot(slot);
+    if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    if (enable && !s->hasOrderModel()) return fail(TDP_ERR_ARGUMENT, "tdp_enable_order_model: no model installed");
+    s->enableOrderModel(enable != 0);
+    return 0;
+}
+
+}  // extern "C"

@@ -121,6 +121,8 @@ struct EngineParams {
     const int *cancel;        // slot cancel flag (device)
     unsigned long long timeLimitNs;  // every warp stops (error kErrDeadline) after this long
     int sparse;                      // same-cycle pair enumeration allowed (n <= 32)
+    const uint16_t *order;           // per-instance root child order (learned), or null
+    int orderStride;
 };
 
 }  // namespace tdp

@@ -10,6 +10,7 @@
 #include <map>
 #include <vector>
 
+#include "mlp.h"
 #include "search_kernel.cuh"
 
 namespace tdp {
@@ -121,6 +122,15 @@ SearchSlot::~SearchSlot() {
     cudaFreeHost(hOut_);
     cudaFreeHost(hRules_);
     cudaFreeHost(hCancelValue_);
+    for (int l = 0; l < 4; ++l) {
+        cudaFree(dW_[l]);
+        cudaFree(dB_[l]);
+    }
+    cudaFree(dX_);
+    for (int l = 0; l < 3; ++l) cudaFree(dH_[l]);
+    cudaFree(dScores_);
+    cudaFree(dOrder_);
+    cudaFree(dMlpErr_);
     cudaEventDestroy(evStart_);
     cudaEventDestroy(evStop_);
     cudaStreamDestroy(stream_);
@@ -272,6 +282,8 @@ void SearchSlot::launchClass(int cls, int offset, int count) {
     P.cancel = dCancel_;
     P.timeLimitNs = (unsigned long long)(std::max(0.001, cfg_.time_limit_s) * 1e9);
     P.sparse = cfg_.sparse_enumeration;
+    P.order = (cls == 0 && orderedLaunch_) ? dOrder_ : nullptr;
+    P.orderStride = combinations3(32);
 
     int blocksPerSM = 0;
     const int threads = dev::kWarpsPerBlock * 32;
@@ -315,6 +327,12 @@ int SearchSlot::runStaged(std::string &err) {
     check(cudaEventRecord(evStart_, stream_), "event");
     // Both size classes are enqueued back to back; their control blocks are read after.
     launched_[0] = launched_[1] = false;
+    orderedLaunch_ = false;
+    if (orderEnabled_ && hasOrderModel() && countSmall_ > 0) {
+        const int rc = computeRootOrder(countSmall_, err);
+        if (rc != 0) return rc;
+        orderedLaunch_ = true;
+    }
     launchClass(0, 0, countSmall_);
     launchClass(1, countSmall_, count_ - countSmall_);
     check(cudaEventRecord(evStop_, stream_), "event");
@@ -328,6 +346,15 @@ int SearchSlot::runStaged(std::string &err) {
     float ms = 0.f;
     check(cudaEventElapsedTime(&ms, evStart_, evStop_), "elapsed");
     kernelMs_ = ms;
+    if (orderedLaunch_) {
+        int mlpErr = 0;
+        check(cudaMemcpy(&mlpErr, dMlpErr_, sizeof(int), cudaMemcpyDeviceToHost), "read mlp error");
+        if (mlpErr) {
+            check(cudaMemset(dMlpErr_, 0, sizeof(int)), "reset mlp error");
+            err = "ordering model: tensor-core pipeline wait timed out";
+            return TDP_ERR_DEVICE;
+        }
+    }
     if (deviceError_ != 0) {
         err = deviceError_ == kErrDeadline ? "GPU sorting search exceeded its device time limit"
                                            : "GPU sorting search device error (spin limit)";
@@ -375,6 +402,73 @@ int SearchSlot::searchBatch(const tdp_instance *instances, int count, float minR
     rc = runStaged(err);
     if (rc != 0) return rc;
     return fetch(results);
+}
+
+int SearchSlot::setOrderModel(const uint16_t *w1, const float *b1, const uint16_t *w2, const float *b2,
+                              const uint16_t *w3, const float *b3, const uint16_t *w4, const float *b4,
+                              std::string &err) {
+    (void)err;
+    check(cudaSetDevice(device_), "cudaSetDevice");
+    const int rows[4] = {mlp::kHidden, mlp::kHidden, mlp::kHidden, mlp::kTriplesPadded};
+    const int cols[4] = {mlp::kFeatures, mlp::kHidden, mlp::kHidden, mlp::kHidden};
+    const int realRows[4] = {mlp::kHidden, mlp::kHidden, mlp::kHidden, mlp::kTriples};
+    const uint16_t *w[4] = {w1, w2, w3, w4};
+    const float *b[4] = {b1, b2, b3, b4};
+    for (int l = 0; l < 4; ++l) {
+        if (!dW_[l]) check(cudaMalloc(&dW_[l], (size_t)rows[l] * cols[l] * 2), "cudaMalloc(order weights)");
+        if (!dB_[l]) check(cudaMalloc(&dB_[l], (size_t)rows[l] * sizeof(float)), "cudaMalloc(order bias)");
+        check(cudaMemset(dW_[l], 0, (size_t)rows[l] * cols[l] * 2), "clear weights");
+        check(cudaMemset(dB_[l], 0, (size_t)rows[l] * sizeof(float)), "clear bias");
+        check(cudaMemcpy(dW_[l], w[l], (size_t)realRows[l] * cols[l] * 2, cudaMemcpyHostToDevice), "upload weights");
+        check(cudaMemcpy(dB_[l], b[l], (size_t)realRows[l] * sizeof(float), cudaMemcpyHostToDevice), "upload bias");
+    }
+    if (!dMlpErr_) {
+        check(cudaMalloc(&dMlpErr_, sizeof(int)), "cudaMalloc(mlp error)");
+        check(cudaMemset(dMlpErr_, 0, sizeof(int)), "clear mlp error");
+    }
+    return 0;
+}
+
+// Scores every staged n <= 32 root with the MLP (tensor-core GEMMs on the slot stream, in
+// chunks) and sorts its children by descending score into dOrder_.
+int SearchSlot::computeRootOrder(int count, std::string &err) {
+    constexpr int kChunk = 8192;
+    const int stride = combinations3(32);
+    if (count > orderCap_) {
+        cudaFree(dOrder_);
+        dOrder_ = nullptr;
+        check(cudaMalloc(&dOrder_, (size_t)count * stride * sizeof(uint16_t)), "cudaMalloc(order)");
+        orderCap_ = count;
+    }
+    if (!dX_) {
+        check(cudaMalloc(&dX_, (size_t)kChunk * mlp::kFeatures * 2), "cudaMalloc(features)");
+        for (int l = 0; l < 3; ++l) check(cudaMalloc(&dH_[l], (size_t)kChunk * mlp::kHidden * 2), "cudaMalloc(hidden)");
+        check(cudaMalloc(&dScores_, (size_t)kChunk * mlp::kTriplesPadded * sizeof(float)), "cudaMalloc(scores)");
+    }
+    const uint8_t *base = reinterpret_cast<const uint8_t *>(dIn_);
+    for (int off = 0; off < count; off += kChunk) {
+        const int rows = std::min(kChunk, count - off);
+        const uint8_t *rec = base + (size_t)off * sizeof(InstanceIn);
+        mlp::build_features(rec + offsetof(InstanceIn, spi), rec + offsetof(InstanceIn, pi),
+                            rec + offsetof(InstanceIn, n), (int)sizeof(InstanceIn), (int)sizeof(InstanceIn), rows,
+                            static_cast<__nv_bfloat16 *>(dX_), stream_);
+        const void *in = dX_;
+        int k = mlp::kFeatures;
+        for (int l = 0; l < 3; ++l) {
+            if (mlp::gemm_bf16(in, dW_[l], rows, mlp::kHidden, k, dB_[l], 1, dH_[l], 0, mlp::kHidden, dMlpErr_,
+                               stream_, err) != 0)
+                return TDP_ERR_CUDA;
+            in = dH_[l];
+            k = mlp::kHidden;
+        }
+        if (mlp::gemm_bf16(in, dW_[3], rows, mlp::kTriplesPadded, mlp::kHidden, dB_[3], 0, dScores_, 1,
+                           mlp::kTriplesPadded, dMlpErr_, stream_, err) != 0)
+            return TDP_ERR_CUDA;
+        mlp::order_by_score(dScores_, mlp::kTriplesPadded, rec + offsetof(InstanceIn, n), (int)sizeof(InstanceIn),
+                            rows, dOrder_ + (size_t)off * stride, stride, stream_);
+    }
+    check(cudaGetLastError(), "ordering model launch");
+    return 0;
 }
 
 tdp_stats SearchSlot::stats() const {

@@ -46,10 +46,17 @@ public:
     tdp_engine_config &config() { return cfg_; }
     int stagedCount() const { return count_; }
 
+    // Learned root ordering (n <= 32 instances of a batch).
+    int setOrderModel(const uint16_t *w1, const float *b1, const uint16_t *w2, const float *b2, const uint16_t *w3,
+                      const float *b3, const uint16_t *w4, const float *b4, std::string &err);
+    bool hasOrderModel() const { return dW_[0] != nullptr; }
+    void enableOrderModel(bool on) { orderEnabled_ = on; }
+
 private:
     void ensureCapacity(int instances, int rules);
     void launchClass(int cls, int offset, int count);
     void wait();
+    int computeRootOrder(int count, std::string &err);
 
     int device_ = 0;
     int numSMs_ = 1;
@@ -85,6 +92,17 @@ private:
     int deviceError_ = 0;
     int launches_ = 0;
     bool launched_[2] = {false, false};
+
+    // ordering model: weights (bf16 [out x in]) and biases, inference scratch, root orders
+    void *dW_[4] = {nullptr, nullptr, nullptr, nullptr};
+    float *dB_[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool orderEnabled_ = false;
+    void *dX_ = nullptr, *dH_[3] = {nullptr, nullptr, nullptr};
+    float *dScores_ = nullptr;
+    uint16_t *dOrder_ = nullptr;
+    int orderCap_ = 0;
+    int *dMlpErr_ = nullptr;
+    bool orderedLaunch_ = false;
 };
 
 }  // namespace tdp

@@ -508,7 +508,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         for (int h = 0; h < NW; ++h) S.words[f][h * 32 + lane] = w[h];
         uint64_t satMask = shfl64(ruleReg, f + 1);
         uint64_t expMask = shfl64(ruleReg, 16 + f + 1);
-        SparseFrame sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse);
+        // The root of an instance with a learned order enumerates its children in that order
+        // (dense mode, index space = positions in the order).
+        const uint16_t *rootOrder = (P.order && NW == 1) ? P.order + (size_t)inst * (size_t)P.orderStride : nullptr;
+        SparseFrame sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse && !(rootOrder && f == 0));
         // A donated range is in the units of its frame's mode (the receiver derives the same
         // mode from the same node); a root covers every child.
         if (kind == 2) end = sf.on ? sf.np : T;
@@ -537,7 +540,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                     for (int h = 0; h < NW; ++h) w[h] = S.words[f][h * 32 + lane];
                     satMask = shfl64(ruleReg, f + 1);
                     expMask = shfl64(ruleReg, 16 + f + 1);
-                    sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse);
+                    sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse && !(rootOrder && f == 0));
                     continue;
                 }
                 if (++poll >= P.pollInterval) {
@@ -668,7 +671,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                     const int t = cursor + lane;
                     cursor += 32;
                     valid = t < end;
-                    tr = valid ? __ldg(trip + t) : 0u;
+                    tr = valid ? __ldg(trip + ((rootOrder && f == 0) ? (int)__ldg(rootOrder + t) : t)) : 0u;
                     a = w_pi(gather<NW>(w, tri_i(tr)));
                     b = w_pi(gather<NW>(w, tri_j(tr)));
                     c = w_pi(gather<NW>(w, tri_k(tr)));
@@ -721,7 +724,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                 tr = (r < ps.p) ? pack_triple(r, ps.p, ps.q)
                                 : (r < ps.q) ? pack_triple(ps.p, r, ps.q) : pack_triple(ps.p, ps.q, r);
             } else {
-                tr = __ldg(trip + chunk + l);
+                const int t = chunk + l;
+                tr = __ldg(trip + ((rootOrder && f == 0) ? (int)__ldg(rootOrder + t) : t));
             }
             if (lane == f) {
                 fCursor = cursor;
@@ -764,7 +768,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
             for (int h = 0; h < NW; ++h) S.words[f][h * 32 + lane] = w[h];
             satMask = shfl64(ruleReg, f + 1);
             expMask = shfl64(ruleReg, 16 + f + 1);
-            sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse);
+            sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse && !(rootOrder && f == 0));
             cursor = 0;
             end = sf.on ? sf.np : T;
             pending = 0u;

@@ -1,0 +1,156 @@
+"""GPU numerics of the move-ordering MLP kernels against a plain PyTorch fp32 reference, and
+verdict identity of the learned-order search."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+R1375 = float(np.float32(2) / np.float32(1.375))
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+@pytest.mark.parametrize("m,n,k,relu,fp32", [(300, 256, 1088, True, False), (128, 5632, 256, False, True),
+                                             (64, 256, 256, True, True), (1000, 512, 64, False, True)])
+def test_tcgen05_gemm_matches_torch_fp32(native_lib, torch_cuda, m, n, k, relu, fp32):
+    """bf16 inputs, fp32 accumulation: |err| <= 2e-3 * (|ref| + 1) against torch's fp32
+    product of the same bf16-rounded operands (bf16 output: 1e-2)."""
+    import torch
+    from tdp1375_b200 import order_model
+    g = torch.Generator(device="cpu").manual_seed(m * 7 + n)
+    a = (torch.randn(m, k, generator=g) * 0.5).to(torch.bfloat16).cuda()
+    b = (torch.randn(n, k, generator=g) * 0.5).to(torch.bfloat16).cuda()
+    bias = torch.randn(n, generator=g).cuda()
+    out = order_model.gemm(a, b, bias, relu=relu, out_fp32=fp32)
+    torch.cuda.synchronize()
+    assert native_lib.tdp_mlp_error() == 0
+    ref = a.float() @ b.float().T + bias
+    if relu:
+        ref = torch.relu(ref)
+    tol = 2e-3 if fp32 else 1e-2
+    err = (out.float() - ref).abs() / (ref.abs() + 1.0)
+    assert float(err.max()) <= tol, float(err.max())
+
+
+def test_features_match_numpy(native_lib, torch_cuda):
+    import torch
+    from tdp1375_b200 import order_model
+    from tdp1375_b200.cases import config_cases
+    cases = list(config_cases(5, 16))
+    spi = np.zeros((16, 64), np.uint8)
+    pi = np.zeros((16, 64), np.uint8)
+    ns = np.zeros(16, np.uint8)
+    for r, (p, s, _, _) in enumerate(cases):
+        spi[r, :len(s)] = s
+        pi[r, :len(p)] = p
+        ns[r] = len(p)
+    x = order_model.features(torch.from_numpy(spi).cuda(), torch.from_numpy(pi).cuda(),
+                             torch.from_numpy(ns).cuda()).float().cpu().numpy()
+    for r in range(16):
+        n = int(ns[r])
+        pos = {int(pi[r, q]): q for q in range(n)}
+        want = np.zeros(1088, np.float32)
+        for i in range(n):
+            want[i * 32 + pos[int(spi[r, pi[r, i]])]] = 1.0
+        seen = set()
+        for s in range(n):
+            if s in seen:
+                continue
+            length, cur = 0, s
+            while cur not in seen:
+                seen.add(cur)
+                cur = int(spi[r, cur])
+                length += 1
+            want[1024 + length - 1] += 1.0
+        assert np.array_equal(x[r], want), r
+
+
+def test_softmax_xent_matches_torch(native_lib, torch_cuda):
+    import ctypes
+    import torch
+    from tdp1375_b200 import order_model
+    rows = 8
+    logits = torch.randn(rows, 5632, device="cuda")
+    ns = torch.tensor([32, 30, 24, 18, 12, 32, 9, 27], dtype=torch.uint8, device="cuda")
+    valid = torch.zeros(rows, 5456, dtype=torch.bool)
+    lex = order_model.LEX32
+    for r in range(rows):
+        n = int(ns[r])
+        ids = lex[:n, :n, :n][lex[:n, :n, :n] >= 0]
+        valid[r, torch.from_numpy(ids.astype(np.int64))] = True
+    valid = valid.cuda()
+    target = torch.tensor([int(torch.nonzero(valid[r])[r % 3 * 5]) for r in range(rows)], dtype=torch.int32,
+                          device="cuda")
+    dl = torch.empty(rows, 5632, dtype=torch.bfloat16, device="cuda")
+    loss = torch.empty(rows, device="cuda")
+    L = order_model.lib()
+    rc = L.tdp_mlp_softmax_xent(ctypes.c_void_p(logits.data_ptr()), 5632, ctypes.c_void_p(ns.data_ptr()),
+                                ctypes.c_void_p(target.data_ptr()), rows, ctypes.c_void_p(dl.data_ptr()),
+                                ctypes.c_void_p(loss.data_ptr()), ctypes.c_void_p(0))
+    assert rc == 0
+    torch.cuda.synchronize()
+    masked = logits[:, :5456].masked_fill(~valid, float("-inf"))
+    ref_loss = torch.nn.functional.cross_entropy(masked, target.long(), reduction="none")
+    assert torch.allclose(loss, ref_loss, atol=1e-4, rtol=1e-4)
+    ref_grad = (torch.softmax(masked, 1) - torch.nn.functional.one_hot(target.long(), 5456)) / rows
+    assert torch.allclose(dl[:, :5456].float(), ref_grad, atol=2e-4)
+    assert float(dl[:, 5456:].float().abs().max()) == 0.0
+
+
+def test_order_kernel_sorts_by_score(native_lib, torch_cuda):
+    import ctypes
+    import torch
+    from tdp1375_b200 import order_model
+    rows = 4
+    scores = torch.randn(rows, 5632, device="cuda")
+    ns = torch.tensor([32, 17, 5, 24], dtype=torch.uint8, device="cuda")
+    order = torch.zeros(rows, 5456, dtype=torch.int16, device="cuda")
+    rc = order_model.lib().tdp_mlp_order(ctypes.c_void_p(scores.data_ptr()), 5632, ctypes.c_void_p(ns.data_ptr()),
+                                         rows, ctypes.c_void_p(order.data_ptr()), 5456, ctypes.c_void_p(0))
+    assert rc == 0
+    torch.cuda.synchronize()
+    sc = scores.cpu().numpy()
+    got = order.cpu().numpy().view(np.uint16)
+    for r in range(rows):
+        n = int(ns[r])
+        trip = [(i, j, k) for i in range(n) for j in range(i + 1, n) for k in range(j + 1, n)]
+        keyed = sorted(range(len(trip)), key=lambda t: (-sc[r, order_model.LEX32[trip[t]]], t))
+        assert list(got[r, :len(trip)]) == keyed
+
+
+def test_training_reduces_loss_and_ordering_keeps_verdicts(native_lib, torch_cuda):
+    """Trains briefly on solution pairs of the plain search, installs the model and checks
+    that the ordered batched search returns the plain search's verdicts (and valid sequences)."""
+    from oracle import oracle
+    from tdp1375_b200 import GPUSortingSearch, make_instances, search_batch
+    from tdp1375_b200 import order_model
+    from tdp1375_b200.cases import config_cases
+    GPUSortingSearch(1, 1, 256 << 20, 1 << 22)
+    try:
+        train_cases = [c[:3] for c in config_cases(1, 400, start=50_000)]
+        res = search_batch(0, make_instances(train_cases, 8, False), len(train_cases), R1375)
+        spi, pi, ns, tgt = order_model.solution_pairs(train_cases, res)
+        assert len(tgt) > 500
+        model = order_model.OrderModel()
+        stats = order_model.train(model, spi, pi, ns, tgt, epochs=6, batch=512, lr=2e-3)
+        assert native_lib.tdp_mlp_error() == 0
+        assert stats.last_loss < stats.first_loss
+        eval_cases = [c[:3] for c in config_cases(5, 64)]
+        inst = make_instances(eval_cases, 8, False)
+        plain = search_batch(0, inst, len(eval_cases), R1375)
+        plain_status = [r.status for r in plain]
+        model.install(0, enable=True)
+        ordered = search_batch(0, inst, len(eval_cases), R1375)
+        assert [r.status for r in ordered] == plain_status
+        for (p, s, e), r in zip(eval_cases, ordered):
+            if r.status == 1:
+                pos = [[r.positions[3 * d + t] for t in range(3)] for d in range(r.depth)]
+                ok, _ = oracle.replay_positions(list(p), list(s), pos, e, R1375, False)
+                assert ok
+    finally:
+        GPUSortingSearch.destroySlots()
