@@ -43,6 +43,7 @@ assert ctypes.sizeof(Instance) == 136 and ctypes.sizeof(Result) == 208
 
 u8p = ctypes.POINTER(ctypes.c_uint8)
 i32p = ctypes.POINTER(ctypes.c_int32)
+vp = ctypes.c_void_p
 
 # name -> (restype, argtypes); this list is the ABI surface that the CPU test checks.
 SIGNATURES = {
@@ -63,6 +64,20 @@ SIGNATURES = {
     "tdp_last_stats": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Stats)]),
     "tdp_get_engine_config": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(EngineConfig)]),
     "tdp_set_engine_config": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(EngineConfig)]),
+    # move-ordering MLP (device pointers, stream as void*)
+    "tdp_mlp_gemm": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp,
+                                    ctypes.c_int, ctypes.c_int, vp]),
+    "tdp_mlp_features": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp, vp]),
+    "tdp_mlp_softmax_xent": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, vp]),
+    "tdp_mlp_transpose": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp, vp]),
+    "tdp_mlp_relu_backward": (ctypes.c_int, [vp, vp, ctypes.c_int64, vp]),
+    "tdp_mlp_column_sums": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp, vp]),
+    "tdp_mlp_adam": (ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int64, ctypes.c_float, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_float, ctypes.c_int, vp]),
+    "tdp_mlp_order": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, vp]),
+    "tdp_mlp_error": (ctypes.c_int, []),
+    "tdp_set_order_model": (ctypes.c_int, [ctypes.c_int] + [vp] * 8),
+    "tdp_enable_order_model": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
 }
 
 _lib = None

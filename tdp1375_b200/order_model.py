@@ -39,25 +39,8 @@ def _lex32_table() -> np.ndarray:
 LEX32 = _lex32_table()
 
 
-def _setup(lib):
-    vp, fp, u8p, i32p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.c_void_p, ctypes.c_void_p
-    lib.tdp_mlp_gemm.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int,
-                                 ctypes.c_int, vp]
-    lib.tdp_mlp_features.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
-    lib.tdp_mlp_softmax_xent.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, vp]
-    lib.tdp_mlp_transpose.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
-    lib.tdp_mlp_relu_backward.argtypes = [vp, vp, ctypes.c_int64, vp]
-    lib.tdp_mlp_column_sums.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
-    lib.tdp_mlp_adam.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
-                                 ctypes.c_float, ctypes.c_int, vp]
-    lib.tdp_mlp_order.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp, ctypes.c_int, vp]
-    lib.tdp_set_order_model.argtypes = [ctypes.c_int] + [vp] * 8
-    lib.tdp_enable_order_model.argtypes = [ctypes.c_int, ctypes.c_int]
-    return lib
-
-
 def lib():
-    return _setup(native.load())
+    return native.load()
 
 
 def _check(rc):
