@@ -1,6 +1,7 @@
 // Permutation filter host entry (pi_filter.cu).
 #pragma once
 
+#include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <string>
