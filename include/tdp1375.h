@@ -41,7 +41,7 @@ const char *tdp_last_error(void);
 
 /* Replaces initGpuSortSlots (slot_manager.cu:62-98), JNI initSlots (jni_sorter.cu:25-34).
  * Destroys previous slots, then creates total_slots slots; slot s lives on device
- * s % devices_count.  queue_bytes_budget (bytes) bounds the donation pool; dedup_table_size
+ * s % devices_count.  queue_bytes_budget (bytes) bounds the work-donation mailboxes; dedup_table_size
  * is the transposition-table capacity in entries (rounded up to a power of two). */
 int tdp_init_slots(int total_slots, int devices_count, int64_t queue_bytes_budget, int dedup_table_size);
 
@@ -119,10 +119,10 @@ typedef struct tdp_engine_config {
     int32_t blocks_per_sm;   /* 0 = occupancy maximum */
     int32_t poll_interval;   /* chunks between flag polls / donation checks */
     int32_t tight_bound;     /* 1 = verdict-preserving strengthened prune, 0 = reference prune only */
-    int32_t task_capacity;   /* donation pool entries (<= queue budget) */
+    int32_t task_capacity;   /* read-only: warp mailboxes for work donation (sized from the queue budget) */
     double time_limit_s;     /* device deadline per launch */
     int32_t sparse_enumeration; /* 1 = same-cycle pair enumeration where -2 children are useless */
-    int32_t reserved;
+    int32_t use_cuda_graph;     /* 1 = tdp_batch_run replays one captured CUDA graph per prepared batch */
 } tdp_engine_config;
 
 int tdp_get_engine_config(int slot, tdp_engine_config *cfg);
@@ -131,15 +131,15 @@ int tdp_set_engine_config(int slot, const tdp_engine_config *cfg);
 int tdp_device_count(void);
 
 /* ---- learned move ordering (no counterpart in the reference) ------------------------
- * A 1088 -> 256 -> 256 -> 256 -> 5456 BF16 MLP (fp32 accumulation on the tcgen05 tensor
+ * A 1088 -> 256 -> 256 -> 256 -> 4960 BF16 MLP (fp32 accumulation on the tcgen05 tensor
  * cores) scores the (i,j,k) triples of a configuration with n <= 32; the batched search then
  * expands each instance's root children in descending score order.  Ordering only permutes
  * children: verdicts are unchanged.  The entry points below take DEVICE pointers and a
  * cudaStream_t (as void*); they are the building blocks of inference and training. */
 #define TDP_MLP_FEATURES 1088
 #define TDP_MLP_HIDDEN 256
-#define TDP_MLP_TRIPLES 5456
-#define TDP_MLP_TRIPLES_PADDED 5632
+#define TDP_MLP_TRIPLES 4960
+#define TDP_MLP_TRIPLES_PADDED 5120
 
 /* C[m x n] = A[m x k] * B[n x k]^T (+bias[n]) (ReLU if relu); A, B bf16 row-major, k % 8 == 0,
  * 16-byte aligned; out bf16 (out_fp32 = 0) or fp32 with row stride ldo. */
@@ -160,7 +160,7 @@ int tdp_mlp_order(const float *scores, int ld, const uint8_t *n, int count, uint
 int tdp_mlp_error(void);
 
 /* Installs the ordering model on a slot (host arrays: bf16 weights as uint16 bits in the
- * torch.nn.Linear [out, in] layout, fp32 biases; w4 has 5456 rows).  enable = 0 keeps the
+ * torch.nn.Linear [out, in] layout, fp32 biases; w4 has 4960 rows).  enable = 0 keeps the
  * weights but searches in plain order. */
 int tdp_set_order_model(int slot, const uint16_t *w1, const float *b1, const uint16_t *w2, const float *b2,
                         const uint16_t *w3, const float *b3, const uint16_t *w4, const float *b4);

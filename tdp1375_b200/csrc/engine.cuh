@@ -40,8 +40,9 @@ struct alignas(16) InstanceOut {
     uint32_t moves[16];           // packed positions (pack_triple), depth entries
 };
 
-// A donated piece of work: the children [lo, hi) (lexicographic triple indices) of one
-// node at `depth`, with the move path that reached it (208 B).
+// A donated piece of work: the children [lo, hi) of one node at `depth` (in the index
+// space of that node's enumeration mode; hi = 0xFFFF means all children), with the move
+// path that reached it.  flags bit 0: the node has not been expanded yet (208 B).
 struct alignas(16) Task {
     uint32_t inst;
     uint8_t depth;
@@ -50,7 +51,7 @@ struct alignas(16) Task {
     uint8_t reserved1;
     uint16_t lo;
     uint16_t hi;
-    uint32_t reserved2;
+    uint32_t flags;
     uint32_t path[16];
     uint8_t spi[64];
     uint8_t pi[64];
@@ -68,13 +69,12 @@ enum EngineStat : int {
     kStatCount
 };
 
-// Launch-wide control block, zeroed before every launch.  Fields that thousands of warps
-// poll live on separate 128-byte lines so one hot line does not serialise the others.
+// Launch-wide control block, zeroed before every launch.  Fields that many warps touch
+// live on separate 128-byte lines.
 struct alignas(128) EngineCtl {
-    int taskTop;  // line 0: donation pool
-    int taskLock;
-    int pad0[30];
-    int hungry;  // line 1: idle warps
+    unsigned ringHead;  // line 0: idle-warp ring, consumer side (donors)
+    int pad0[31];
+    unsigned ringTail;  // line 1: idle-warp ring, producer side (idle warps)
     int pad1[31];
     int nextInstance;  // line 2: instance admission / completion
     int doneCount;
@@ -83,6 +83,14 @@ struct alignas(128) EngineCtl {
     int error;
     int pad3[30];
     unsigned long long stats[kStatCount];  // line 4
+};
+
+// Per-warp mailbox: a donor that dequeued this warp from the idle ring writes a Task here
+// and then releases flag = 1; only the owning warp polls it.
+struct alignas(256) Mailbox {
+    Task task;
+    uint32_t flag;
+    uint32_t pad[11];
 };
 
 enum EngineError : int {
@@ -113,10 +121,12 @@ struct EngineParams {
     const uint32_t *triples;  // lexicographic (i,j,k) per n at offset combinations4(n)
     void *table;
     uint32_t tableMask;       // entries - 1 (entries of this launch's layout)
-    uint32_t generation;
+    const uint32_t *generation;  // device word: this launch's table generation (1..4094)
     uint32_t *doneBits;
-    Task *tasks;
-    int taskCap;
+    Mailbox *mail;            // one per warp of the grid
+    uint32_t *ringSeq;        // idle-warp ring: per-slot lap word (zeroed per launch)
+    uint32_t *ringWid;
+    uint32_t ringMask;        // capacity - 1, capacity >= warps in the grid
     EngineCtl *ctl;
     const int *cancel;        // slot cancel flag (device)
     unsigned long long timeLimitNs;  // every warp stops (error kErrDeadline) after this long

@@ -12,8 +12,8 @@ namespace mlp {
 
 constexpr int kFeatures = 1088;     // 32x32 adjacency bits + 64-bin cycle-length histogram
 constexpr int kHidden = 256;
-constexpr int kTriples = 5456;      // C(32,3)
-constexpr int kTriplesPadded = 5632;  // 22 tiles of 256
+constexpr int kTriples = 4960;        // C(32,3)
+constexpr int kTriplesPadded = 5120;  // 20 tiles of 256
 
 struct GemmParams {
     int M, N, K;
@@ -24,6 +24,9 @@ struct GemmParams {
     int ldo;
     int *error;
 };
+
+// One-time set-up of the GEMM (shared-memory attribute, tensor-map encoder); 0 on success.
+int prepare(std::string &err);
 
 // C = A[M x K] * B[N x K]^T (+ bias, ReLU); out is bf16 (outFp32 = 0) or fp32, row stride ldo.
 int gemm_bf16(const void *A, const void *B, int M, int N, int K, const float *bias, int relu, void *out, int outFp32,

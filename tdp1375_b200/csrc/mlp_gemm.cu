@@ -273,6 +273,19 @@ bool make_map(CUtensorMap *map, const void *base, int rows, int cols, int boxRow
 
 }  // namespace
 
+int prepare(std::string &err) {
+    static std::once_flag attrOnce;
+    static cudaError_t attrErr = cudaSuccess;
+    std::call_once(attrOnce, [] {
+        attrErr = cudaFuncSetAttribute(gemm_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    });
+    if (attrErr != cudaSuccess) {
+        err = std::string("gemm set-up: ") + cudaGetErrorString(attrErr);
+        return -3;
+    }
+    return encode_fn(err) ? 0 : -1;
+}
+
 int gemm_bf16(const void *A, const void *B, int M, int N, int K, const float *bias, int relu, void *out, int outFp32,
               int ldo, int *errorFlag, cudaStream_t stream, std::string &err) {
     if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !out || !errorFlag) {
@@ -281,10 +294,7 @@ int gemm_bf16(const void *A, const void *B, int M, int N, int K, const float *bi
     }
     CUtensorMap ma, mb;
     if (!make_map(&ma, A, M, K, BM, err) || !make_map(&mb, B, N, K, BN, err)) return -1;
-    static std::once_flag attrOnce;
-    std::call_once(attrOnce, [] {
-        cudaFuncSetAttribute(gemm_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    });
+    if (prepare(err) != 0) return -3;
     GemmParams p{};
     p.M = M;
     p.N = N;

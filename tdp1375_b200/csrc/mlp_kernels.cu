@@ -80,9 +80,9 @@ __global__ void softmax_xent_kernel(const float *logits, int ld, const uint8_t *
     for (int c = threadIdx.x; c < kTriples; c += blockDim.x) {
         // decode c -> (i,j,k) by counting
         int rem = c, i = 0;
-        while (rem >= (31 - i) * (30 - i) / 2) rem -= (31 - i) * (30 - i) / 2, ++i;
+        while (i < 29 && rem >= (31 - i) * (30 - i) / 2) rem -= (31 - i) * (30 - i) / 2, ++i;
         int j = i + 1;
-        while (rem >= 31 - j) rem -= 31 - j, ++j;
+        while (j < 30 && rem >= 31 - j) rem -= 31 - j, ++j;
         const int k = j + 1 + rem;
         if (k < n) mx = fmaxf(mx, row[c]);
     }
@@ -100,9 +100,9 @@ __global__ void softmax_xent_kernel(const float *logits, int ld, const uint8_t *
     float sum = 0.f;
     for (int c = threadIdx.x; c < kTriples; c += blockDim.x) {
         int rem = c, i = 0;
-        while (rem >= (31 - i) * (30 - i) / 2) rem -= (31 - i) * (30 - i) / 2, ++i;
+        while (i < 29 && rem >= (31 - i) * (30 - i) / 2) rem -= (31 - i) * (30 - i) / 2, ++i;
         int j = i + 1;
-        while (rem >= 31 - j) rem -= 31 - j, ++j;
+        while (j < 30 && rem >= 31 - j) rem -= 31 - j, ++j;
         const int k = j + 1 + rem;
         if (k < n) sum += __expf(row[c] - mx);
     }
@@ -122,9 +122,9 @@ __global__ void softmax_xent_kernel(const float *logits, int ld, const uint8_t *
         float g = 0.f;
         if (c < kTriples) {
             int rem = c, i = 0;
-            while (rem >= (31 - i) * (30 - i) / 2) rem -= (31 - i) * (30 - i) / 2, ++i;
+            while (i < 29 && rem >= (31 - i) * (30 - i) / 2) rem -= (31 - i) * (30 - i) / 2, ++i;
             int j = i + 1;
-            while (rem >= 31 - j) rem -= 31 - j, ++j;
+            while (j < 30 && rem >= 31 - j) rem -= 31 - j, ++j;
             const int k = j + 1 + rem;
             if (k < n) g = __expf(row[c] - mx) / sum - (c == tgt ? 1.f : 0.f);
         }
@@ -191,9 +191,9 @@ __global__ void __launch_bounds__(1024) order_kernel(const float *scores, int ld
         if (t < T) {
             // n-space lexicographic index t -> (i, j, k)
             int rem = t, i = 0;
-            while (rem >= (n - 1 - i) * (n - 2 - i) / 2) rem -= (n - 1 - i) * (n - 2 - i) / 2, ++i;
+            while (i < n - 3 && rem >= (n - 1 - i) * (n - 2 - i) / 2) rem -= (n - 1 - i) * (n - 2 - i) / 2, ++i;
             int j = i + 1;
-            while (rem >= n - 1 - j) rem -= n - 1 - j, ++j;
+            while (j < n - 2 && rem >= n - 1 - j) rem -= n - 1 - j, ++j;
             const int kk = j + 1 + rem;
             k = scores[(size_t)s * ld + lex32(i, j, kk)];
             idx = (uint16_t)t;

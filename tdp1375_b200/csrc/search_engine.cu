@@ -96,11 +96,24 @@ SearchSlot::SearchSlot(int device, int64_t queueBytesBudget, int dedupTableSize)
     tableEntries32_ = round_pow2((uint64_t)std::max(dedupTableSize, 1024));
     check(cudaMalloc(&dTable_, (size_t)tableEntries32_ * 32), "cudaMalloc(dedup table)");
     check(cudaMemset(dTable_, 0, (size_t)tableEntries32_ * 32), "cudaMemset(dedup table)");
-    const int64_t fromBudget = queueBytesBudget / (int64_t)sizeof(Task);
-    taskCap_ = (int)std::max<int64_t>(1024, std::min<int64_t>(fromBudget, 1 << 16));
-    cfg_.task_capacity = taskCap_;
-    check(cudaMalloc(&dTasks_, (size_t)taskCap_ * sizeof(Task)), "cudaMalloc(tasks)");
+    // One mailbox per warp of the largest grid this slot launches, and an idle-warp ring with
+    // at least as many slots.  The queue budget of the reference (bytes for node queues)
+    // bounds the mailbox area; the default budgets leave room for every resident warp.
+    int maxBlocksPerSM = 0;
+    check(cudaDeviceGetAttribute(&maxBlocksPerSM, cudaDevAttrMaxBlocksPerMultiprocessor, device), "blocks per SM");
+    const int64_t warps = (int64_t)numSMs_ * std::min(maxBlocksPerSM, 8) * dev::kWarpsPerBlock;
+    const int64_t byBudget = std::max<int64_t>(queueBytesBudget, 0) / (int64_t)sizeof(Mailbox);
+    mailboxes_ = (int)std::max<int64_t>((int64_t)dev::kWarpsPerBlock * numSMs_,
+                                        std::min<int64_t>(warps, std::max<int64_t>(byBudget, 1)));
+    uint32_t ring = 1;
+    while (ring < (uint32_t)mailboxes_) ring <<= 1;
+    ringSize_ = ring;
+    cfg_.task_capacity = mailboxes_;
+    check(cudaMalloc(&dMail_, (size_t)mailboxes_ * sizeof(Mailbox)), "cudaMalloc(mailboxes)");
+    check(cudaMalloc(&dRing_, (size_t)ringSize_ * 2 * sizeof(uint32_t)), "cudaMalloc(idle ring)");
     check(cudaMalloc(&dCtl_, sizeof(EngineCtl)), "cudaMalloc(ctl)");
+    check(cudaMalloc(&dGen_, sizeof(uint32_t)), "cudaMalloc(generation)");
+    check(cudaHostAlloc(&hGen_, 2 * sizeof(uint32_t), cudaHostAllocPortable), "cudaHostAlloc(generation)");
     check(cudaHostAlloc(&hCtl_, 2 * sizeof(EngineCtl), cudaHostAllocPortable), "cudaHostAlloc(ctl)");
     ensureCapacity(1, 1);
 }
@@ -110,7 +123,8 @@ SearchSlot::~SearchSlot() {
     if (stream_) cudaStreamSynchronize(stream_);
     if (cancelStream_) cudaStreamSynchronize(cancelStream_);
     cudaFree(dTable_);
-    cudaFree(dTasks_);
+    cudaFree(dMail_);
+    cudaFree(dRing_);
     cudaFree(dCtl_);
     cudaFree(dIn_);
     cudaFree(dOut_);
@@ -131,6 +145,9 @@ SearchSlot::~SearchSlot() {
     cudaFree(dScores_);
     cudaFree(dOrder_);
     cudaFree(dMlpErr_);
+    dropGraph();
+    cudaFree(dGen_);
+    cudaFreeHost(hGen_);
     cudaEventDestroy(evStart_);
     cudaEventDestroy(evStop_);
     cudaStreamDestroy(stream_);
@@ -186,7 +203,16 @@ void SearchSlot::cancel() {
 }
 
 // Validates and stages instances (n <= 32 first, then n > 32) with their rule tables.
+void SearchSlot::dropGraph() {
+    if (graphExec_) cudaGraphExecDestroy(graphExec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    graphExec_ = nullptr;
+    graph_ = nullptr;
+    graphValid_ = false;
+}
+
 int SearchSlot::stage(const tdp_instance *instances, int count, float minRate, std::string &err) {
+    graphValid_ = false;
     order_.clear();
     order_.reserve(count);
     for (int pass = 0; pass < 2; ++pass)
@@ -254,16 +280,13 @@ int SearchSlot::stage(const tdp_instance *instances, int count, float minRate, s
 
 void SearchSlot::launchClass(int cls, int offset, int count) {
     if (count <= 0) return;
-    const int layout = cls;  // 0: 32-byte entries, 1: 64-byte entries
-    if (generation_ >= kMaxGeneration || layout != lastLayout_) {
-        check(cudaMemsetAsync(dTable_, 0, (size_t)tableEntries32_ * 32, stream_), "clear dedup table");
-        generation_ = 0;
-        lastLayout_ = layout;
-    }
-    ++generation_;
+    // the generation word is copied from hGen_[cls], which runStaged set before this run
+    check(cudaMemcpyAsync(dGen_, hGen_ + cls, sizeof(uint32_t), cudaMemcpyHostToDevice, stream_), "generation");
     check(cudaMemsetAsync(dCtl_, 0, sizeof(EngineCtl), stream_), "reset ctl");
     check(cudaMemsetAsync(dOut_ + offset, 0, (size_t)count * sizeof(InstanceOut), stream_), "reset results");
     check(cudaMemsetAsync(dDone_, 0, (size_t)((count + 31) / 32) * sizeof(uint32_t), stream_), "reset done bits");
+    check(cudaMemsetAsync(dMail_, 0, (size_t)mailboxes_ * sizeof(Mailbox), stream_), "reset mailboxes");
+    check(cudaMemsetAsync(dRing_, 0, (size_t)ringSize_ * sizeof(uint32_t), stream_), "reset idle ring");
 
     EngineParams P{};
     P.in = dIn_ + offset;
@@ -274,10 +297,12 @@ void SearchSlot::launchClass(int cls, int offset, int count) {
     P.triples = triples_;
     P.table = dTable_;
     P.tableMask = (cls == 0 ? tableEntries32_ : tableEntries32_ / 2) - 1u;
-    P.generation = generation_;
+    P.generation = dGen_;
     P.doneBits = dDone_;
-    P.tasks = dTasks_;
-    P.taskCap = std::min(taskCap_, cfg_.task_capacity > 0 ? cfg_.task_capacity : taskCap_);
+    P.mail = dMail_;
+    P.ringSeq = dRing_;
+    P.ringWid = dRing_ + ringSize_;
+    P.ringMask = ringSize_ - 1u;
     P.ctl = dCtl_;
     P.cancel = dCancel_;
     P.timeLimitNs = (unsigned long long)(std::max(0.001, cfg_.time_limit_s) * 1e9);
@@ -296,7 +321,8 @@ void SearchSlot::launchClass(int cls, int offset, int count) {
     }
     if (cfg_.blocks_per_sm > 0) blocksPerSM = std::min(blocksPerSM, cfg_.blocks_per_sm);
     blocksPerSM = std::max(1, blocksPerSM);
-    const int grid = numSMs_ * blocksPerSM;
+    // every warp of the grid needs a mailbox
+    const int grid = std::min(numSMs_ * blocksPerSM, mailboxes_ / dev::kWarpsPerBlock);
     if (cls == 0) {
         dev::search_engine_kernel<1><<<grid, threads, 0, stream_>>>(P);
     } else {
@@ -319,22 +345,67 @@ void SearchSlot::wait() {
     }
 }
 
+// Everything one batch run puts on the stream (root ordering, both size classes, control
+// block read-back); captured once into a CUDA graph when use_cuda_graph is set.
+void SearchSlot::enqueueRun(std::string &err, int &rc) {
+    rc = 0;
+    if (orderEnabled_ && hasOrderModel() && countSmall_ > 0) {
+        rc = computeRootOrder(countSmall_, err);
+        if (rc != 0) return;
+        orderedLaunch_ = true;
+    }
+    launchClass(0, 0, countSmall_);
+    launchClass(1, countSmall_, count_ - countSmall_);
+}
+
 int SearchSlot::runStaged(std::string &err) {
     check(cudaSetDevice(device_), "cudaSetDevice");
     deviceError_ = 0;
     launches_ = 0;
     std::fill(std::begin(statsAccum_), std::end(statsAccum_), 0ull);
+    // Table generations: one per size class per run.  On wrap-around, or when the entry
+    // layout changes, the table is cleared (outside any graph).
+    for (int cls = 0; cls < 2; ++cls) {
+        const int n = cls == 0 ? countSmall_ : count_ - countSmall_;
+        if (n <= 0) continue;
+        if (generation_ >= kMaxGeneration || cls != lastLayout_) {
+            check(cudaMemsetAsync(dTable_, 0, (size_t)tableEntries32_ * 32, stream_), "clear dedup table");
+            generation_ = 0;
+            lastLayout_ = cls;
+        }
+        hGen_[cls] = ++generation_;
+    }
+    if (orderEnabled_ && hasOrderModel() && countSmall_ > 0) prepareOrderBuffers(countSmall_);
     check(cudaEventRecord(evStart_, stream_), "event");
-    // Both size classes are enqueued back to back; their control blocks are read after.
     launched_[0] = launched_[1] = false;
     orderedLaunch_ = false;
-    if (orderEnabled_ && hasOrderModel() && countSmall_ > 0) {
-        const int rc = computeRootOrder(countSmall_, err);
+    int rc = 0;
+    if (cfg_.use_cuda_graph) {
+        if (!graphValid_) {
+            dropGraph();
+            check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+            enqueueRun(err, rc);
+            cudaGraph_t g = nullptr;
+            const cudaError_t endErr = cudaStreamEndCapture(stream_, &g);
+            if (rc != 0) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            check(endErr, "end capture");
+            graph_ = g;
+            check(cudaGraphInstantiate(&graphExec_, graph_, 0), "instantiate graph");
+            graphValid_ = true;
+        } else {
+            launched_[0] = countSmall_ > 0;
+            launched_[1] = count_ - countSmall_ > 0;
+            launches_ = (launched_[0] ? 1 : 0) + (launched_[1] ? 1 : 0);
+            orderedLaunch_ = orderEnabled_ && hasOrderModel() && countSmall_ > 0;
+        }
+        check(cudaGraphLaunch(graphExec_, stream_), "graph launch");
+    } else {
+        enqueueRun(err, rc);
         if (rc != 0) return rc;
-        orderedLaunch_ = true;
     }
-    launchClass(0, 0, countSmall_);
-    launchClass(1, countSmall_, count_ - countSmall_);
     check(cudaEventRecord(evStop_, stream_), "event");
     wait();
     for (int cls = 0; cls < 2; ++cls) {
@@ -426,13 +497,18 @@ int SearchSlot::setOrderModel(const uint16_t *w1, const float *b1, const uint16_
         check(cudaMalloc(&dMlpErr_, sizeof(int)), "cudaMalloc(mlp error)");
         check(cudaMemset(dMlpErr_, 0, sizeof(int)), "clear mlp error");
     }
+    // one-time GEMM set-up (kernel attributes, tensor-map encoder) outside any capture
+    if (mlp::prepare(err) != 0) return TDP_ERR_CUDA;
+    graphValid_ = false;
     return 0;
 }
 
 // Scores every staged n <= 32 root with the MLP (tensor-core GEMMs on the slot stream, in
 // chunks) and sorts its children by descending score into dOrder_.
-int SearchSlot::computeRootOrder(int count, std::string &err) {
-    constexpr int kChunk = 8192;
+constexpr int kOrderChunk = 8192;
+
+// Buffers of the ordering pipeline; allocated before any graph capture.
+void SearchSlot::prepareOrderBuffers(int count) {
     const int stride = combinations3(32);
     if (count > orderCap_) {
         cudaFree(dOrder_);
@@ -441,10 +517,16 @@ int SearchSlot::computeRootOrder(int count, std::string &err) {
         orderCap_ = count;
     }
     if (!dX_) {
-        check(cudaMalloc(&dX_, (size_t)kChunk * mlp::kFeatures * 2), "cudaMalloc(features)");
-        for (int l = 0; l < 3; ++l) check(cudaMalloc(&dH_[l], (size_t)kChunk * mlp::kHidden * 2), "cudaMalloc(hidden)");
-        check(cudaMalloc(&dScores_, (size_t)kChunk * mlp::kTriplesPadded * sizeof(float)), "cudaMalloc(scores)");
+        check(cudaMalloc(&dX_, (size_t)kOrderChunk * mlp::kFeatures * 2), "cudaMalloc(features)");
+        for (int l = 0; l < 3; ++l)
+            check(cudaMalloc(&dH_[l], (size_t)kOrderChunk * mlp::kHidden * 2), "cudaMalloc(hidden)");
+        check(cudaMalloc(&dScores_, (size_t)kOrderChunk * mlp::kTriplesPadded * sizeof(float)), "cudaMalloc(scores)");
     }
+}
+
+int SearchSlot::computeRootOrder(int count, std::string &err) {
+    constexpr int kChunk = kOrderChunk;
+    const int stride = combinations3(32);
     const uint8_t *base = reinterpret_cast<const uint8_t *>(dIn_);
     for (int off = 0; off < count; off += kChunk) {
         const int rows = std::min(kChunk, count - off);

@@ -50,13 +50,17 @@ public:
     int setOrderModel(const uint16_t *w1, const float *b1, const uint16_t *w2, const float *b2, const uint16_t *w3,
                       const float *b3, const uint16_t *w4, const float *b4, std::string &err);
     bool hasOrderModel() const { return dW_[0] != nullptr; }
-    void enableOrderModel(bool on) { orderEnabled_ = on; }
+    void enableOrderModel(bool on) {
+        orderEnabled_ = on;
+        graphValid_ = false;
+    }
 
 private:
     void ensureCapacity(int instances, int rules);
     void launchClass(int cls, int offset, int count);
     void wait();
     int computeRootOrder(int count, std::string &err);
+    void prepareOrderBuffers(int count);
 
     int device_ = 0;
     int numSMs_ = 1;
@@ -72,8 +76,10 @@ private:
     uint32_t tableEntries32_ = 0;
     uint32_t generation_ = 0;
     int lastLayout_ = -1;
-    Task *dTasks_ = nullptr;
-    int taskCap_ = 0;
+    Mailbox *dMail_ = nullptr;
+    int mailboxes_ = 0;
+    uint32_t *dRing_ = nullptr;  // lap words then warp ids
+    uint32_t ringSize_ = 0;
     EngineCtl *dCtl_ = nullptr;
     EngineCtl *hCtl_ = nullptr;  // two snapshots: one per size class
 
@@ -86,7 +92,7 @@ private:
     std::vector<int> order_;
     int count_ = 0, countSmall_ = 0;
 
-    tdp_engine_config cfg_{0, 16, 1, 0, 120.0, 1, 0};
+    tdp_engine_config cfg_{0, 8, 1, 0, 120.0, 1, 0};
     unsigned long long statsAccum_[kStatCount] = {};
     double kernelMs_ = 0.0;
     int deviceError_ = 0;
@@ -103,6 +109,14 @@ private:
     int orderCap_ = 0;
     int *dMlpErr_ = nullptr;
     bool orderedLaunch_ = false;
+
+    // generation word (device) fed from pinned host memory, so a captured graph replays
+    uint32_t *dGen_ = nullptr, *hGen_ = nullptr;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t graphExec_ = nullptr;
+    bool graphValid_ = false;
+    void enqueueRun(std::string &err, int &rc);
+    void dropGraph();
 };
 
 }  // namespace tdp

@@ -20,8 +20,10 @@
 //     cycle length) so a child's odd-cycle count is an O(1) delta (tdp_math.cuh) instead
 //     of an O(n) recount, and a descent rebuilds the cycle tables with pointer jumping
 //     over warp shuffles;
-//   * idle warps register as hungry; busy warps split the unexplored triple range of
-//     their shallowest frame into a Task in a global pool (work stealing by donation);
+//   * once every instance is admitted, an idle warp registers its id in a lock-free ring and
+//     polls only its own mailbox line; a busy warp that sees waiting warps dequeues one and
+//     writes a Task straight into its mailbox: half the unexplored range of its shallowest
+//     frame, or an admitted child it has not descended into yet (work donation);
 //   * an instance ends when its last task finishes (outstanding counter), so there is
 //     no global termination scan and no queue to overflow;
 //   * the pruning rule is looked up in host-built bit tables (exact float32 semantics);
@@ -200,8 +202,8 @@ struct LaneStats {
 
 // Transposition-table admission (sorting_search.cu:261-298 semantics, per instance).
 template <int KW>
-__device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t tag, const uint64_t (&key)[KW],
-                                            uint64_t h, uint32_t depth, LaneStats &ls) {
+__device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t generation, uint32_t tag,
+                                            const uint64_t (&key)[KW], uint64_t h, uint32_t depth, LaneStats &ls) {
     auto *table = reinterpret_cast<DedupEntry<KW> *>(P.table);
     const uint32_t base = (uint32_t)(h >> 24) & P.tableMask & ~7u;
     ++ls.probes;
@@ -225,7 +227,7 @@ __device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t tag,
                 }
                 return true;
             }
-        } else if (t == 0u || (t != kTagWriting && (t >> kInstanceBits) != P.generation)) {
+        } else if (t == 0u || (t != kTagWriting && (t >> kInstanceBits) != generation)) {
             freeMask |= 1u << q;
         }
     }
@@ -262,22 +264,62 @@ __device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t tag,
     return true;
 }
 
-__device__ __forceinline__ bool lock_acquire(EngineCtl *ctl) {
+// Idle-warp ring: a bounded lock-free multi-producer/multi-consumer queue of warp ids.  Slot
+// s carries a lap word d = seq - s (zero-initialised): d == lap means free for the enqueue
+// of that lap, d == lap + 1 means it holds an id.  The ring has at least as many slots as
+// the grid has warps and a warp registers at most once at a time, so an enqueue never
+// finds its slot held by an earlier lap for longer than a dequeue in progress.
+__device__ __forceinline__ bool ring_enqueue(const EngineParams &P, uint32_t wid) {
+    const uint32_t pos = atomicAdd(&P.ctl->ringTail, 1u);
+    const uint32_t slot = pos & P.ringMask, lap = pos & ~P.ringMask;
     for (int it = 0; it < kSpinLimit; ++it) {
-        if (atomicCAS(&ctl->taskLock, 0, 1) == 0) {
-            __threadfence();
+        if (ld_acquire_u32(P.ringSeq + slot) == lap) {
+            P.ringWid[slot] = wid;
+            st_release_u32(P.ringSeq + slot, lap + 1u);
             return true;
         }
-        __nanosleep(64);
+        __nanosleep(32);
     }
-    atomicExch(&ctl->error, kErrSpinLimit);
-    atomicExch(&ctl->stop, 1);
+    atomicExch(&P.ctl->error, kErrSpinLimit);
+    atomicExch(&P.ctl->stop, 1);
     return false;
 }
 
-__device__ __forceinline__ void lock_release(EngineCtl *ctl) {
-    __threadfence();
-    atomicExch(&ctl->taskLock, 0);
+// Returns a registered idle warp id, or -1 when the ring is empty (or the race was lost).
+__device__ __forceinline__ int ring_dequeue(const EngineParams &P) {
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        const uint32_t h = ld_relaxed_u32(&P.ctl->ringHead);
+        const uint32_t slot = h & P.ringMask, lap = h & ~P.ringMask;
+        const uint32_t d = ld_acquire_u32(P.ringSeq + slot);
+        if (d == lap + 1u) {
+            if (atomicCAS(&P.ctl->ringHead, h, h + 1u) == h) {
+                const uint32_t w = ld_relaxed_u32(P.ringWid + slot);
+                st_release_u32(P.ringSeq + slot, lap + P.ringMask + 1u);
+                return (int)w;
+            }
+        } else if ((int)(d - (lap + 1u)) < 0) {
+            return -1;  // not filled yet: nobody is waiting at this position
+        }
+    }
+    return -1;
+}
+
+// Children words (spi/pi fields only; tables are rebuilt by the caller) of the move that
+// takes positions (i, j, k), i.e. symbols a, b, c with cycle words wa, wb, wc.
+template <int NW>
+__device__ __forceinline__ void apply_move(const uint32_t (&w)[NW], uint32_t (&out)[NW], int lane, uint32_t i,
+                                           uint32_t j, uint32_t k, uint32_t a, uint32_t b, uint32_t c, uint32_t wa,
+                                           uint32_t wb, uint32_t wc) {
+#pragma unroll
+    for (int h = 0; h < NW; ++h) {
+        const uint32_t x = (uint32_t)(lane + 32 * h);
+        uint32_t s = w_spi(w[h]);
+        if (x == a) s = w_spi(wc);
+        if (x == b) s = w_spi(wa);
+        if (x == c) s = w_spi(wb);
+        const uint32_t src = (uint32_t)block_swap_src((int)x, (int)i, (int)j, (int)k);
+        out[h] = s | (w_pi(gather<NW>(w, src)) << 6);
+    }
 }
 
 // Same-cycle pair enumeration.  When a frame's children can neither succeed nor be
@@ -370,56 +412,50 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
     WarpShared<NW> &S = smem[threadIdx.x >> 5];
     EngineCtl *ctl = P.ctl;
     const unsigned long long deadline = global_time_ns() + P.timeLimitNs;
+    const uint32_t generation = __ldcg(P.generation);
 
     if (lane < kStatCount) S.stats[lane] = 0ull;
     __syncwarp();
     LaneStats ls;
-    bool hungry = false;
-    int backoff = 256;
+    const uint32_t gw = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    bool registered = false;
+    int backoff = 64;
     int idleRound = 0;
     bool stopAll = false;
 
     while (!stopAll) {
         // ---------------------------------------------------------------- get work
+        // Before the last instance is admitted an idle warp admits the next instance; after
+        // that it registers once in the idle ring and polls only its own mailbox line.
         int kind = 0, idx = 0;
         if (lane == 0) {
-            // Idle warps read only the donation line every round; the admission, completion
-            // and stop lines every 8th round (busy warps poll stop/cancel themselves).
-            const bool full = hungry ? ((++idleRound & 7) == 0) : true;
-            bool quit = false;
-            if (full) {
-                const int stopFlag = ld_relaxed_s32(&ctl->stop);
-                const int cancelFlag = ld_relaxed_s32(P.cancel);
-                const bool late = global_time_ns() > deadline;
-                if (late && !(stopFlag | cancelFlag)) {
-                    atomicExch(&ctl->error, kErrDeadline);
-                    atomicExch(&ctl->stop, 1);
-                }
-                quit = (stopFlag | cancelFlag) || late;
-            }
-            if (quit) {
-                kind = -1;
-            } else {
-                if (ld_relaxed_s32(&ctl->taskTop) > 0) {
-                    if (lock_acquire(ctl)) {
-                        volatile int *top = &ctl->taskTop;
-                        const int t = *top;
-                        if (t > 0) {
-                            *top = t - 1;
-                            idx = t - 1;
-                            kind = 1;
-                        } else {
-                            lock_release(ctl);
-                        }
-                    } else {
-                        kind = -1;
+            if (registered && ld_acquire_u32(&P.mail[gw].flag) != 0u) kind = 1;
+            if (kind == 0) {
+                const bool full = registered ? ((++idleRound & 7) == 0) : true;
+                if (full) {
+                    const int stopFlag = ld_relaxed_s32(&ctl->stop);
+                    const int cancelFlag = ld_relaxed_s32(P.cancel);
+                    const bool late = global_time_ns() > deadline;
+                    if (late && !(stopFlag | cancelFlag)) {
+                        atomicExch(&ctl->error, kErrDeadline);
+                        atomicExch(&ctl->stop, 1);
                     }
+                    if ((stopFlag | cancelFlag) || late) kind = -1;
                 }
-                if (kind == 0 && full && ld_relaxed_s32(&ctl->nextInstance) < P.count) {
-                    const int i = atomicAdd(&ctl->nextInstance, 1);
-                    if (i < P.count) {
-                        kind = 2;
-                        idx = i;
+                if (kind == 0 && !registered) {
+                    if (ld_relaxed_s32(&ctl->nextInstance) < P.count) {
+                        const int i = atomicAdd(&ctl->nextInstance, 1);
+                        if (i < P.count) {
+                            kind = 2;
+                            idx = i;
+                        }
+                    }
+                    if (kind == 0) {
+                        if (ring_enqueue(P, gw)) {
+                            registered = true;
+                        } else {
+                            kind = -1;
+                        }
                     }
                 }
                 if (kind == 0 && full && ld_relaxed_s32(&ctl->doneCount) >= P.count) kind = -1;
@@ -429,15 +465,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         idx = __shfl_sync(kFull, idx, 0);
         if (kind < 0) break;
         if (kind == 0) {
-            if (!hungry && lane == 0) atomicAdd(&ctl->hungry, 1);
-            hungry = true;
             __nanosleep(backoff);
-            backoff = min(backoff * 2, 32768);
+            backoff = min(backoff * 2, 2048);
             continue;
         }
-        if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
-        hungry = false;
-        backoff = 256;
+        backoff = 64;
         idleRound = 0;
 
         // ---------------------------------------------------------------- set up
@@ -447,16 +479,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         uint32_t fMove = 0;
         unsigned long long tNodes = 0, tChildren = 0;
         if (kind == 1) {
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(P.tasks + idx);
+            __threadfence();  // every lane reads the task only after lane 0 observed the flag
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(&P.mail[gw].task);
             for (int q = lane; q < 52; q += 32) S.staging[q] = __ldcg(src + q);
             __syncwarp();
-            if (lane == 0) lock_release(ctl);
-            if (lane == 0) ++S.stats[kStatTaskPops];
+            if (lane == 0) {
+                // the mailbox is free again before this warp can re-register
+                *reinterpret_cast<volatile uint32_t *>(&P.mail[gw].flag) = 0u;
+                __threadfence();
+                ++S.stats[kStatTaskPops];
+            }
+            registered = false;
             inst = S.staging[0];
             baseDepth = (int)(S.staging[1] & 0xFFu);
             even = (int)((S.staging[1] >> 8) & 0xFFu);
             lo = (int)(S.staging[2] & 0xFFFFu);
             hi = (int)(S.staging[2] >> 16);
+            if (S.staging[3] & 1u) tNodes = 1;
             if (lane < baseDepth) fMove = S.staging[4 + lane];
             const uint8_t *bytes = reinterpret_cast<const uint8_t *>(S.staging);
             const int n = P.in[inst].n;
@@ -476,7 +515,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
             baseDepth = 0;
             even = I->even0;
             lo = 0;
-            hi = combinations3(I->n);
+            hi = 0xFFFF;
             const int n = I->n;
 #pragma unroll
             for (int h = 0; h < NW; ++h) {
@@ -488,7 +527,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         const int n = P.in[inst].n;
         const int T = combinations3(n);
         const uint32_t *trip = P.triples + combinations4(n);
-        const uint32_t tag = (P.generation << kInstanceBits) | inst;
+        const uint32_t tag = (generation << kInstanceBits) | inst;
         const RuleTable *rt = P.rules + P.in[inst].rule;
         const uint64_t ruleReg = (lane < 16) ? rt->sat[lane] : rt->expand[lane - 16];
 
@@ -513,8 +552,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         const uint16_t *rootOrder = (P.order && NW == 1) ? P.order + (size_t)inst * (size_t)P.orderStride : nullptr;
         SparseFrame sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse && !(rootOrder && f == 0));
         // A donated range is in the units of its frame's mode (the receiver derives the same
-        // mode from the same node); a root covers every child.
-        if (kind == 2) end = sf.on ? sf.np : T;
+        // mode from the same node); hi = 0xFFFF covers every child.
+        if (hi == 0xFFFF) end = sf.on ? sf.np : T;
 
         // outcome: 0 subtree exhausted, 1 instance found (here or elsewhere), 2 launch stop
         int outcome = 0;
@@ -551,8 +590,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                         const int stopFlag = ld_relaxed_s32(&ctl->stop);
                         const int cancelFlag = ld_relaxed_s32(P.cancel);
                         const int state = ld_relaxed_s32(&P.out[inst].state);
-                        const int hg = ld_relaxed_s32(&ctl->hungry);
-                        const int top = ld_relaxed_s32(&ctl->taskTop);
+                        const uint32_t rt = ld_relaxed_u32(&ctl->ringTail);
+                        const uint32_t rh = ld_relaxed_u32(&ctl->ringHead);
                         const bool late = global_time_ns() > deadline;
                         if (stopFlag | cancelFlag) {
                             act = 2;
@@ -562,7 +601,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                             act = 2;
                         } else if (state == kStateFound) {
                             act = 1;
-                        } else if (hg > 0 && top < hg) {
+                        } else if (rt != rh) {
                             act = 3;
                         }
                     }
@@ -573,45 +612,101 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                     }
                     if (act == 3) {
                         // ------------------------------------------------ donate
+                        // Candidates: the shallowest frame with >= 2 unevaluated chunks
+                        // (split its range), or a shallower frame holding admitted children
+                        // not yet descended into (hand over one of them as a fresh node).
                         const int step = sf.on ? 1 : 32;
                         int remChunks = 0;
-                        if (lane >= baseDepth && lane < f) remChunks = (fEnd - fCursor + fStep - 1) / fStep;
-                        if (lane == f) remChunks = (end - cursor + step - 1) / step;
+                        uint32_t pend = 0u;
+                        if (lane >= baseDepth && lane < f) {
+                            remChunks = (fEnd - fCursor + fStep - 1) / fStep;
+                            pend = fPending;
+                        }
+                        if (lane == f) {
+                            remChunks = (end - cursor + step - 1) / step;
+                            pend = pending;
+                        }
                         const unsigned big = __ballot_sync(kFull, remChunks >= 2);
+                        const unsigned held = __ballot_sync(kFull, pend != 0u);
                         const unsigned some = __ballot_sync(kFull, remChunks > 0 && lane < f);
-                        const int g = big ? (__ffs(big) - 1) : (some ? (__ffs(some) - 1) : -1);
-                        if (g >= 0) {
-                            const int gc = __shfl_sync(kFull, (lane == f) ? cursor : fCursor, g);
-                            const int ge = __shfl_sync(kFull, (lane == f) ? end : fEnd, g);
+                        const int g1 = big ? (__ffs(big) - 1) : 99;
+                        const int gp = held ? (__ffs(held) - 1) : 99;
+                        const int g0 = some ? (__ffs(some) - 1) : 99;
+                        int mode = 0, g = -1;  // 1 range split, 2 pending child, 3 whole range
+                        if (gp < g1 && gp < 99) {
+                            mode = 2;
+                            g = gp;
+                        } else if (g1 < 99) {
+                            mode = 1;
+                            g = g1;
+                        } else if (g0 < 99) {
+                            mode = 3;
+                            g = g0;
+                        }
+                        int target = -1;
+                        if (mode != 0 && lane == 0) target = ring_dequeue(P);
+                        target = __shfl_sync(kFull, target, 0);
+                        if (target >= 0) {
+                            Task *tk = &P.mail[target].task;
                             const int gEven = __shfl_sync(kFull, (lane == f) ? even : fEven, g);
-                            const int gStep = __shfl_sync(kFull, (lane == f) ? step : fStep, g);
-                            const int remg = (ge - gc + gStep - 1) / gStep;
-                            const int keepChunks = (remg >= 2) ? (remg + 1) / 2 : 0;
-                            const int newEnd = min(ge, gc + keepChunks * gStep);
-                            int slot = -1;
-                            if (lane == 0 && newEnd < ge) {
-                                atomicAdd(&P.out[inst].outstanding, 1);
-                                if (lock_acquire(ctl)) {
-                                    volatile int *top = &ctl->taskTop;
-                                    if (*top < P.taskCap) {
-                                        slot = *top;
-                                    } else {
-                                        lock_release(ctl);
+                            uint32_t hdr1, hdr2, hdr3;
+                            if (mode == 2) {
+                                const int gChunk = __shfl_sync(kFull, (lane == f) ? chunk : fChunk, g);
+                                const uint32_t gPend = __shfl_sync(kFull, pend, g);
+                                const int l = __ffs(gPend) - 1;
+                                uint32_t wg[NW];
+#pragma unroll
+                                for (int h = 0; h < NW; ++h) wg[h] = S.words[g][h * 32 + lane];
+                                const uint64_t gSat = shfl64(ruleReg, g + 1);
+                                const uint64_t gExp = shfl64(ruleReg, 16 + g + 1);
+                                const SparseFrame gsf =
+                                    sparse_setup<NW>(wg, n, lane, gEven, gSat, gExp, P.sparse && !(rootOrder && g == 0));
+                                uint32_t ctr;
+                                if (gsf.on) {
+                                    const PairSel ps = sparse_pair(gsf, gChunk);
+                                    ctr = (l < ps.p) ? pack_triple(l, ps.p, ps.q)
+                                                     : (l < ps.q) ? pack_triple(ps.p, l, ps.q)
+                                                                  : pack_triple(ps.p, ps.q, l);
+                                } else {
+                                    const int t = gChunk + l;
+                                    ctr = __ldg(trip + ((rootOrder && g == 0) ? (int)__ldg(rootOrder + t) : t));
+                                }
+                                const uint32_t ci = tri_i(ctr), cj = tri_j(ctr), ck = tri_k(ctr);
+                                const uint32_t ca = w_pi(gather<NW>(wg, ci));
+                                const uint32_t cb = w_pi(gather<NW>(wg, cj));
+                                const uint32_t cc = w_pi(gather<NW>(wg, ck));
+                                const uint32_t cwa = gather<NW>(wg, ca);
+                                const uint32_t cwb = gather<NW>(wg, cb);
+                                const uint32_t cwc = gather<NW>(wg, cc);
+                                const int cEven = gEven + move_delta(cwa, cwb, cwc);
+                                uint32_t cw[NW];
+                                apply_move<NW>(wg, cw, lane, ci, cj, ck, ca, cb, cc, cwa, cwb, cwc);
+#pragma unroll
+                                for (int h = 0; h < NW; ++h) {
+                                    const int x = lane + 32 * h;
+                                    if (x < n) {
+                                        tk->spi[x] = (uint8_t)w_spi(cw[h]);
+                                        tk->pi[x] = (uint8_t)w_pi(cw[h]);
                                     }
                                 }
-                                if (slot < 0) atomicSub(&P.out[inst].outstanding, 1);
-                            }
-                            slot = __shfl_sync(kFull, slot, 0);
-                            if (slot >= 0) {
-                                Task *tk = P.tasks + slot;
-                                if (lane == 0) {
-                                    uint32_t *hdr = reinterpret_cast<uint32_t *>(tk);
-                                    hdr[0] = inst;
-                                    hdr[1] = (uint32_t)g | ((uint32_t)gEven << 8);
-                                    hdr[2] = (uint32_t)newEnd | ((uint32_t)ge << 16);
-                                    hdr[3] = 0u;
-                                }
                                 if (lane < g) tk->path[lane] = fMove;
+                                if (lane == g) tk->path[g] = ctr;
+                                hdr1 = (uint32_t)(g + 1) | ((uint32_t)cEven << 8);
+                                hdr2 = 0xFFFFu << 16;
+                                hdr3 = 1u;
+                                const uint32_t bit = 1u << l;
+                                if (g == f) {
+                                    pending &= ~bit;
+                                } else if (lane == g) {
+                                    fPending &= ~bit;
+                                }
+                            } else {
+                                const int gc = __shfl_sync(kFull, (lane == f) ? cursor : fCursor, g);
+                                const int ge = __shfl_sync(kFull, (lane == f) ? end : fEnd, g);
+                                const int gStep = __shfl_sync(kFull, (lane == f) ? step : fStep, g);
+                                const int remg = (ge - gc + gStep - 1) / gStep;
+                                const int keepChunks = (mode == 1) ? (remg + 1) / 2 : 0;
+                                const int newEnd = min(ge, gc + keepChunks * gStep);
 #pragma unroll
                                 for (int h = 0; h < NW; ++h) {
                                     const int x = lane + 32 * h;
@@ -621,23 +716,34 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                                         tk->pi[x] = (uint8_t)w_pi(wg);
                                     }
                                 }
-                                __threadfence();
-                                __syncwarp();
-                                if (lane == 0) {
-                                    volatile int *top = &ctl->taskTop;
-                                    *top = slot + 1;
-                                    lock_release(ctl);
-                                }
+                                if (lane < g) tk->path[lane] = fMove;
+                                hdr1 = (uint32_t)g | ((uint32_t)gEven << 8);
+                                hdr2 = (uint32_t)newEnd | ((uint32_t)ge << 16);
+                                hdr3 = 0u;
                                 if (g == f) {
                                     end = newEnd;
                                 } else if (lane == g) {
                                     fEnd = newEnd;
                                 }
-                                if (lane == 0) ++S.stats[kStatDonations];
+                            }
+                            if (lane == 0) {
+                                uint32_t *hdr = reinterpret_cast<uint32_t *>(tk);
+                                hdr[0] = inst;
+                                hdr[1] = hdr1;
+                                hdr[2] = hdr2;
+                                hdr[3] = hdr3;
+                                atomicAdd(&P.out[inst].outstanding, 1);
+                            }
+                            __threadfence();
+                            __syncwarp();
+                            if (lane == 0) {
+                                st_release_u32(&P.mail[target].flag, 1u);
+                                ++S.stats[kStatDonations];
                             }
                         }
-                        // The donor keeps at least one chunk of its current frame
-                        // (newEnd > cursor when g == f), so it evaluates it next.
+                        // A range split keeps at least one chunk of the donor's frame and a
+                        // hand-off never touches the current frame's range (its pending mask
+                        // is empty here), so the donor carries on with its next chunk.
                     }
                 }
                 // ---------------------------------------------------- evaluate a chunk
@@ -709,7 +815,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                     set_field<NW>(ck, a, w_spi(wc));
                     set_field<NW>(ck, b, w_spi(wa));
                     set_field<NW>(ck, c, w_spi(wb));
-                    adm = dedup_admit<KW>(P, tag, ck, key_hash<KW>(ck, tag), (uint32_t)(f + 1), ls);
+                    adm = dedup_admit<KW>(P, generation, tag, ck, key_hash<KW>(ck, tag), (uint32_t)(f + 1), ls);
                 }
                 pending = __ballot_sync(kFull, adm);
                 continue;
@@ -750,16 +856,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
             set_field<NW>(key, b, w_spi(wa));
             set_field<NW>(key, c, w_spi(wb));
             uint32_t nw[NW];
-#pragma unroll
-            for (int h = 0; h < NW; ++h) {
-                const uint32_t x = (uint32_t)(lane + 32 * h);
-                uint32_t s = w_spi(w[h]);
-                if (x == a) s = w_spi(wc);
-                if (x == b) s = w_spi(wa);
-                if (x == c) s = w_spi(wb);
-                const uint32_t src = (uint32_t)block_swap_src((int)x, (int)i, (int)j, (int)k);
-                nw[h] = s | (w_pi(gather<NW>(w, src)) << 6);
-            }
+            apply_move<NW>(w, nw, lane, i, j, k, a, b, c, wa, wb, wc);
 #pragma unroll
             for (int h = 0; h < NW; ++h) w[h] = nw[h];
             build_tables<NW>(w, n, lane);
@@ -796,7 +893,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         }
         __syncwarp();
     }
-    if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
 
     // ---------------------------------------------------------------- statistics
     unsigned long long probes = ls.probes, pruned = ls.pruned, inserts = ls.inserts, full = ls.full;  // widen once

@@ -1,8 +1,8 @@
 """Learned move ordering: data generation, training and installation of the BF16 MLP.
 
-The model scores the C(32,3) = 5456 position triples (i<j<k) of a configuration with
+The model scores the C(32,3) = 4960 position triples (i<j<k) of a configuration with
 n <= 32 symbols: 1088 inputs (32x32 adjacency of spi in pi-position coordinates + a 64-bin
-cycle-length histogram), three hidden layers of 256 (ReLU), 5456 outputs.  All matrix
+cycle-length histogram), three hidden layers of 256 (ReLU), 4960 outputs.  All matrix
 products run in the library's tcgen05 GEMM (``tdp_mlp_gemm``); torch only holds device
 memory.  Training pairs are (state, next move) along the solutions the plain search finds;
 the loss is softmax cross-entropy over the triples valid for the state's n.
@@ -21,7 +21,7 @@ import numpy as np
 
 from . import native
 
-FEATURES, HIDDEN, TRIPLES, TRIPLES_PADDED = 1088, 256, 5456, 5632
+FEATURES, HIDDEN, TRIPLES, TRIPLES_PADDED = 1088, 256, 4960, 5120
 LAYERS = [(HIDDEN, FEATURES), (HIDDEN, HIDDEN), (HIDDEN, HIDDEN), (TRIPLES_PADDED, HIDDEN)]
 
 

@@ -15,7 +15,7 @@ def torch_cuda():
     return torch
 
 
-@pytest.mark.parametrize("m,n,k,relu,fp32", [(300, 256, 1088, True, False), (128, 5632, 256, False, True),
+@pytest.mark.parametrize("m,n,k,relu,fp32", [(300, 256, 1088, True, False), (128, 5120, 256, False, True),
                                              (64, 256, 256, True, True), (1000, 512, 64, False, True)])
 def test_tcgen05_gemm_matches_torch_fp32(native_lib, torch_cuda, m, n, k, relu, fp32):
     """bf16 inputs, fp32 accumulation: |err| <= 2e-3 * (|ref| + 1) against torch's fp32
@@ -75,9 +75,9 @@ def test_softmax_xent_matches_torch(native_lib, torch_cuda):
     import torch
     from tdp1375_b200 import order_model
     rows = 8
-    logits = torch.randn(rows, 5632, device="cuda")
+    logits = torch.randn(rows, 5120, device="cuda")
     ns = torch.tensor([32, 30, 24, 18, 12, 32, 9, 27], dtype=torch.uint8, device="cuda")
-    valid = torch.zeros(rows, 5456, dtype=torch.bool)
+    valid = torch.zeros(rows, 4960, dtype=torch.bool)
     lex = order_model.LEX32
     for r in range(rows):
         n = int(ns[r])
@@ -86,20 +86,20 @@ def test_softmax_xent_matches_torch(native_lib, torch_cuda):
     valid = valid.cuda()
     target = torch.tensor([int(torch.nonzero(valid[r])[r % 3 * 5]) for r in range(rows)], dtype=torch.int32,
                           device="cuda")
-    dl = torch.empty(rows, 5632, dtype=torch.bfloat16, device="cuda")
+    dl = torch.empty(rows, 5120, dtype=torch.bfloat16, device="cuda")
     loss = torch.empty(rows, device="cuda")
     L = order_model.lib()
-    rc = L.tdp_mlp_softmax_xent(ctypes.c_void_p(logits.data_ptr()), 5632, ctypes.c_void_p(ns.data_ptr()),
+    rc = L.tdp_mlp_softmax_xent(ctypes.c_void_p(logits.data_ptr()), 5120, ctypes.c_void_p(ns.data_ptr()),
                                 ctypes.c_void_p(target.data_ptr()), rows, ctypes.c_void_p(dl.data_ptr()),
                                 ctypes.c_void_p(loss.data_ptr()), ctypes.c_void_p(0))
     assert rc == 0
     torch.cuda.synchronize()
-    masked = logits[:, :5456].masked_fill(~valid, float("-inf"))
+    masked = logits[:, :4960].masked_fill(~valid, float("-inf"))
     ref_loss = torch.nn.functional.cross_entropy(masked, target.long(), reduction="none")
     assert torch.allclose(loss, ref_loss, atol=1e-4, rtol=1e-4)
-    ref_grad = (torch.softmax(masked, 1) - torch.nn.functional.one_hot(target.long(), 5456)) / rows
-    assert torch.allclose(dl[:, :5456].float(), ref_grad, atol=2e-4)
-    assert float(dl[:, 5456:].float().abs().max()) == 0.0
+    ref_grad = (torch.softmax(masked, 1) - torch.nn.functional.one_hot(target.long(), 4960)) / rows
+    assert torch.allclose(dl[:, :4960].float(), ref_grad, atol=2e-4)
+    assert float(dl[:, 4960:].float().abs().max()) == 0.0
 
 
 def test_order_kernel_sorts_by_score(native_lib, torch_cuda):
@@ -107,11 +107,11 @@ def test_order_kernel_sorts_by_score(native_lib, torch_cuda):
     import torch
     from tdp1375_b200 import order_model
     rows = 4
-    scores = torch.randn(rows, 5632, device="cuda")
+    scores = torch.randn(rows, 5120, device="cuda")
     ns = torch.tensor([32, 17, 5, 24], dtype=torch.uint8, device="cuda")
-    order = torch.zeros(rows, 5456, dtype=torch.int16, device="cuda")
-    rc = order_model.lib().tdp_mlp_order(ctypes.c_void_p(scores.data_ptr()), 5632, ctypes.c_void_p(ns.data_ptr()),
-                                         rows, ctypes.c_void_p(order.data_ptr()), 5456, ctypes.c_void_p(0))
+    order = torch.zeros(rows, 4960, dtype=torch.int16, device="cuda")
+    rc = order_model.lib().tdp_mlp_order(ctypes.c_void_p(scores.data_ptr()), 5120, ctypes.c_void_p(ns.data_ptr()),
+                                         rows, ctypes.c_void_p(order.data_ptr()), 4960, ctypes.c_void_p(0))
     assert rc == 0
     torch.cuda.synchronize()
     sc = scores.cpu().numpy()
