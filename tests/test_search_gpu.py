@@ -156,3 +156,32 @@ def test_cancel_stops_a_long_search(gpu_searcher):
     assert errors and (errors[0] == "GPU sorting search cancelled" or errors[0] == "finished")
     # the slot is usable afterwards
     assert GPUSortingSearch.searchForSortingSeq(list(range(5)), list(range(5)), 5, R1375, 3, True, 1) == []
+
+
+def test_cuda_graph_replay_matches_direct_launch(gpu_searcher, oracle):
+    """tdp_batch_run with use_cuda_graph replays one captured graph (root ordering off):
+    two replays give the verdicts of a direct launch, with fresh table generations."""
+    import ctypes
+    from tdp1375_b200 import api, make_instances, native
+    from tdp1375_b200.cases import config_cases
+    lib = native.load()
+    cases = [c[:3] for c in config_cases(1, 48)]
+    inst = make_instances(cases, 11, True)
+    direct = run_batch(cases, 11, True, R1375, slot=1)
+    cfg = api.engine_config(1)
+    graph_cfg = native.EngineConfig(cfg.blocks_per_sm, cfg.poll_interval, cfg.tight_bound, cfg.task_capacity,
+                                    cfg.time_limit_s, cfg.sparse_enumeration, 1)
+    api.set_engine_config(1, graph_cfg)
+    try:
+        assert lib.tdp_batch_prepare(1, inst, len(cases), ctypes.c_float(R1375)) == 0, native.last_error()
+        for _ in range(2):
+            assert lib.tdp_batch_run(1) == 0, native.last_error()
+            res = (native.Result * len(cases))()
+            assert lib.tdp_batch_results(1, res) == 0
+            assert [r.status for r in res] == [r.status for r in direct]
+            for (pi, spi, even), r in zip(cases, res):
+                if r.status == 1:
+                    ok, _ = oracle.replay_positions(list(pi), list(spi), positions(r), even, R1375, True)
+                    assert ok
+    finally:
+        api.set_engine_config(1, cfg)
