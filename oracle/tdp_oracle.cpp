@@ -480,3 +480,95 @@ int oracle_pi_filter_keep(const uint8_t *pi, int n, const uint8_t *cycle, int cy
 }
 
 }  // extern "C"
+
+// ---- extension filter (batched use of the pi_filter.cu:55-115 predicates) -----------------
+// Candidates of a base configuration (spi, pi) over n symbols, in this order:
+//   A. for every a<b<c (lexicographic) and orientation o in {0,1}: spi' = spi o rho with
+//      rho = (a b c) (o = 0) or (a c b) (o = 1); pi' = pi; the added cycle is rho;
+//   B. for every 0 <= g1 <= g2 <= g3 <= n (lexicographic) and orientation o: three new
+//      symbols x=n, y=n+1, z=n+2 inserted into pi before original positions g1, g2, g3 (x
+//      first on ties), spi' = spi plus the cycle (x y z) (o = 0) or (x z y) (o = 1).
+// A candidate is kept when the added cycle, as written, is in cyclic order in pi'
+// (pi_filter.cu:132-133), at least one cycle of spi' is oriented (pi_filter.cu:135-142,
+// CommonOperations.java:443-445) and no oriented cycle of spi' admits a 2-move
+// (pi_filter.cu:86-115, CommonOperations.java:406-431).
+namespace {
+
+int comb3(int n) { return n < 3 ? 0 : n * (n - 1) * (n - 2) / 6; }
+
+void decode_triple(int t, int n, int &i, int &j, int &k) {
+    i = 0;
+    while (i < n - 3 && t >= (n - 1 - i) * (n - 2 - i) / 2) t -= (n - 1 - i) * (n - 2 - i) / 2, ++i;
+    j = i + 1;
+    while (j < n - 2 && t >= n - 1 - j) t -= n - 1 - j, ++j;
+    k = j + 1 + t;
+}
+
+bool keep_candidate(const uint8_t *spi, const uint8_t *pi, int n, const uint8_t *added) {
+    uint8_t index[kMaxN + 1], rindex[kMaxN + 1];
+    for (int q = 0; q < n; ++q) index[pi[q]] = static_cast<uint8_t>(q);
+    if (!cyclic_order3(index, added[0], added[1], added[2])) return false;
+    for (int s = 0; s < n; ++s) rindex[s] = static_cast<uint8_t>((n - 1) - index[s]);
+    uint64_t seen = 0;
+    bool anyOriented = false;
+    for (int s = 0; s < n; ++s) {
+        if ((seen >> s) & 1ull) continue;
+        uint8_t cyc[kMaxN + 1], cidx[kMaxN + 1] = {0};
+        int len = 0, cur = s;
+        do {
+            seen |= 1ull << cur;
+            cidx[cur] = static_cast<uint8_t>(len);
+            cyc[len++] = static_cast<uint8_t>(cur);
+            cur = spi[cur];
+        } while (cur != s);
+        if (cyclic_order(rindex, cyc, len)) continue;  // not oriented
+        anyOriented = true;
+        if (has_2_move(index, cyc, cidx, len)) return false;
+    }
+    return anyOriented;
+}
+
+}  // namespace
+
+extern "C" int oracle_extension_count(int n) { return 2 * comb3(n) + 2 * comb3(n + 3); }
+
+extern "C" int64_t oracle_extension_filter(const uint8_t *spi, const uint8_t *pi, int n, uint8_t *keep) {
+    if (n < 3 || n + 3 > kMaxN) return -1;
+    int64_t hits = 0;
+    int e = 0;
+    uint8_t s2[kMaxN + 1], p2[kMaxN + 1], added[3];
+    for (int t = 0; t < comb3(n); ++t)
+        for (int o = 0; o < 2; ++o, ++e) {
+            int a, b, c;
+            decode_triple(t, n, a, b, c);
+            const int r1 = o == 0 ? b : c, r2 = o == 0 ? c : b;  // rho = (a r1 r2)
+            int rho[kMaxN + 1];
+            for (int x = 0; x < n; ++x) rho[x] = x;
+            rho[a] = r1;
+            rho[r1] = r2;
+            rho[r2] = a;
+            for (int x = 0; x < n; ++x) s2[x] = spi[rho[x]];
+            added[0] = a, added[1] = r1, added[2] = r2;
+            keep[e] = keep_candidate(s2, pi, n, added) ? 1 : 0;
+            hits += keep[e];
+        }
+    const int m = n + 3;
+    for (int t = 0; t < comb3(n + 3); ++t)
+        for (int o = 0; o < 2; ++o, ++e) {
+            int i, j, k;
+            decode_triple(t, n + 3, i, j, k);
+            const int g[3] = {i, j - 1, k - 2};
+            int q = 0, w = 0;
+            for (int pos = 0; pos <= n; ++pos) {
+                while (w < 3 && g[w] == pos) p2[q++] = static_cast<uint8_t>(n + w), ++w;
+                if (pos < n) p2[q++] = pi[pos];
+            }
+            for (int x = 0; x < n; ++x) s2[x] = spi[x];
+            const int x = n, y = n + 1, z = n + 2;
+            if (o == 0) s2[x] = y, s2[y] = z, s2[z] = x, added[0] = x, added[1] = y, added[2] = z;
+            else s2[x] = z, s2[z] = y, s2[y] = x, added[0] = x, added[1] = z, added[2] = y;
+            keep[e] = keep_candidate(s2, p2, m, added) ? 1 : 0;
+            hits += keep[e];
+        }
+    return hits;
+}
