@@ -3,8 +3,9 @@
 Workload: 3-permutation configurations of the tdp1375 proof (spi = product of m disjoint
 3-cycles on n = 3m symbols, pi = identity), m ~ U{4..8}, seeded case by case
 (seed 1375 + 2*10**6 + case) over a 100,000-case set; full sorting, ratio 1.375
-(minRate = float32(2)/float32(1.375)), max depth 11, transposition table of 2M entries,
-queue budget 3000 MB, one slot.  A step is one batch of --batch consecutive cases
+(minRate = float32(2)/float32(1.375)), max depth 11, queue budget 3000 MB, one slot.  The
+transposition table holds 2^30 entries (32 GB): a full-sorting m=8 instance inserts ~36M
+states, and a saturated table multiplies the explored nodes (2^27 entries: 15x more nodes).  A step is one batch of --batch consecutive cases
 (step s of rank r covers cases [(s*N + r)*B, (s*N + r + 1)*B) mod 100,000).
 
 value: cases/s with the step's instances already resident in HBM (tdp_batch_prepare before
@@ -29,7 +30,7 @@ sys.path.insert(0, ROOT)
 TOTAL_CASES = 100_000
 CONFIG = 2
 MAX_DEPTH = 11
-DEDUP_ENTRIES = 1 << 21
+DEDUP_ENTRIES = 1 << 30  # 32 GB of 32-byte entries: room for every concurrent m=8 instance
 QUEUE_BYTES = 3000 << 20
 HBM_FALLBACK_GBS = 6650.0
 
@@ -39,7 +40,7 @@ def parse_args():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
-    p.add_argument("--batch", type=int, default=2000)
+    p.add_argument("--batch", type=int, default=40)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--cpu-budget-s", type=float, default=15.0, help="CPU baseline sample length")
     p.add_argument("--cpu-node-limit", type=int, default=3_000_000)

@@ -73,7 +73,7 @@ def test_config1_verdicts_match_oracle(gpu_searcher, oracle):
                 assert ok
 
 
-@pytest.mark.parametrize("full,depth", [(False, 8), (True, 11)])
+@pytest.mark.parametrize("full,depth", [(False, 8), (True, 8)])
 def test_engine_modes_keep_verdicts(gpu_searcher, oracle, full, depth):
     """Single-instance calls, batched calls, and the engine with the tight bound and/or
     the same-cycle pair enumeration switched off all give the same verdicts."""
