@@ -166,6 +166,21 @@ int tdp_set_order_model(int slot, const uint16_t *w1, const float *b1, const uin
                         const uint16_t *w3, const float *b3, const uint16_t *w4, const float *b4);
 int tdp_enable_order_model(int slot, int enable);
 
+/* ---- allocation-free permutation filter (no counterpart in the reference) ------------
+ * For callers that must not allocate device memory: code running while a CUDA stream is
+ * being captured, host runtimes whose own allocator owns the whole device heap, and
+ * real-time hosts that forbid allocation once they are running.  It is the filter of
+ * tdp_pi_filter, but it calls no cudaMalloc/cudaFree: its scratch is a static 156 KB device
+ * array inside this library (held on every GPU that loads it until the process exits), and
+ * rows go to out_device, a DEVICE buffer of max_rows * n bytes owned by the caller.
+ * Limit: n <= 12 ((n-1)! <= 11! candidates); larger n returns TDP_ERR_ARGUMENT.  Work runs
+ * on `stream` (a cudaStream_t, may be null); the call returns after it with the total number
+ * of hits.  The first call on a device looks up the scratch address (cudaGetSymbolAddress):
+ * make that first call outside any stream capture.  All calls share the scratch, so calls
+ * that overlap on the GPU (different streams or threads at once) race; serialise them. */
+int64_t tdp_pi_filter_noalloc(const uint8_t *cycle, int cycle_len, const uint8_t *oriented_triple, int triple_len,
+                              int n, int skip_2move_check, uint8_t *out_device, int64_t max_rows, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

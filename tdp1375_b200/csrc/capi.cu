@@ -349,3 +349,13 @@ int tdp_enable_order_model(int slot, int enable) {
 }
 
 }  // extern "C"
+
+extern "C" int64_t tdp_pi_filter_noalloc(const uint8_t *cycle, int cycle_len, const uint8_t *oriented_triple,
+                                         int triple_len, int n, int skip_2move_check, uint8_t *out_device,
+                                         int64_t max_rows, void *stream) {
+    std::string err;
+    const int64_t rc = tdp::pi_filter_noalloc_run(cycle, cycle_len, oriented_triple, triple_len, n, skip_2move_check,
+                                                  out_device, max_rows, static_cast<cudaStream_t>(stream), err);
+    if (rc >= 0) return rc;
+    return fail(rc == -1 ? TDP_ERR_ARGUMENT : TDP_ERR_CUDA, err);
+}

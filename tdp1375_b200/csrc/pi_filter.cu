@@ -210,6 +210,108 @@ __global__ void __launch_bounds__(kThreads) pi_filter_write_kernel(const FilterA
     }
 }
 
+// ---------------------------------------------------------------- allocation-free variant
+// Scratch of tdp_pi_filter_noalloc, for callers that cannot allocate device memory: slot 0
+// holds the hit total, slots [1, 1+B) the block offsets and [1+B, 1+2B) the block totals,
+// B = number of 4096-rank blocks of 11! candidates (n <= 12).  Every GPU that loads the
+// library keeps these 156 KB until the process exits.  In host code the symbol is only a
+// stand-in: the device address comes from cudaGetSymbolAddress (noalloc_scratch below).
+constexpr int kNoAllocMaxN = 12;
+constexpr unsigned long long kNoAllocMaxRanks = 39916800ull;  // 11!
+constexpr int kNoAllocMaxBlocks = (int)((kNoAllocMaxRanks + kRanksPerBlock - 1) / kRanksPerBlock);
+static __device__ __align__(256) unsigned long long gNoAllocScratch[1 + 2 * kNoAllocMaxBlocks];
+
+// Count pass without per-thread scratch: block totals only.
+__global__ void __launch_bounds__(kThreads) noalloc_count_kernel(const FilterArgs A, unsigned long long *scratch,
+                                                                  int blocks) {
+    uint8_t p[64], index[64], rindex[64];
+    const unsigned long long first = ((unsigned long long)blockIdx.x * kThreads + threadIdx.x) * kRanksPerThread;
+    unsigned hits = 0;
+    if (first < A.total) {
+        unrank(first, A.n, A.fact, p);
+        const unsigned long long last = min(first + kRanksPerThread, A.total);
+        for (unsigned long long r = first; r < last; ++r) {
+            hits += keep(A, p, index, rindex) ? 1u : 0u;
+            next_perm(p, A.n);
+        }
+    }
+    unsigned total;
+    block_exclusive_scan(hits, &total);
+    if (threadIdx.x == 0) scratch[1 + blocks + blockIdx.x] = total;
+}
+
+// One block: block offsets from the block totals; the hit total goes to scratch[0].
+__global__ void __launch_bounds__(kThreads) noalloc_scan_kernel(unsigned long long *scratch, int blocks) {
+    __shared__ unsigned long long running;
+    if (threadIdx.x == 0) running = 0ull;
+    __syncthreads();
+    for (int base = 0; base < blocks; base += kThreads) {
+        const int i = base + (int)threadIdx.x;
+        const unsigned v = (i < blocks) ? (unsigned)scratch[1 + blocks + i] : 0u;
+        unsigned tileTotal;
+        const unsigned prefix = block_exclusive_scan(v, &tileTotal);
+        if (i < blocks) scratch[1 + i] = running + prefix;
+        __syncthreads();
+        if (threadIdx.x == 0) running += tileTotal;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) scratch[0] = running;
+}
+
+// Write pass: each thread recounts its ranks to find its offset inside the block, then
+// re-walks them and stores the kept rows.
+__global__ void __launch_bounds__(kThreads) noalloc_write_kernel(const FilterArgs A, const unsigned long long *scratch,
+                                                                  uint8_t *out, unsigned long long maxRows) {
+    uint8_t p[64], index[64], rindex[64];
+    const unsigned long long first = ((unsigned long long)blockIdx.x * kThreads + threadIdx.x) * kRanksPerThread;
+    const unsigned long long last = min(first + kRanksPerThread, A.total);
+    unsigned hits = 0;
+    if (first < A.total) {
+        unrank(first, A.n, A.fact, p);
+        for (unsigned long long r = first; r < last; ++r) {
+            hits += keep(A, p, index, rindex) ? 1u : 0u;
+            next_perm(p, A.n);
+        }
+    }
+    unsigned total;
+    const unsigned prefix = block_exclusive_scan(hits, &total);
+    if (first >= A.total || hits == 0) return;
+    unsigned long long row = scratch[1 + blockIdx.x] + prefix;
+    if (row >= maxRows) return;
+    unrank(first, A.n, A.fact, p);
+    for (unsigned long long r = first; r < last && row < maxRows; ++r) {
+        if (keep(A, p, index, rindex)) {
+            uint8_t *dst = out + row * (unsigned long long)A.n;
+            for (int i = 0; i < A.n; ++i) dst[i] = p[i];
+            ++row;
+        }
+        next_perm(p, A.n);
+    }
+}
+
+// Device address of gNoAllocScratch for the current device, looked up once per device
+// (with that device current) and cached.
+unsigned long long *noalloc_scratch(std::string &err) {
+    static std::mutex mu;
+    static unsigned long long *addr[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        err = "tdp_pi_filter_noalloc: no current CUDA device";
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, gNoAllocScratch);
+        if (e != cudaSuccess || !ptr) {
+            err = std::string("tdp_pi_filter_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
+            return nullptr;
+        }
+        addr[dev] = static_cast<unsigned long long *>(ptr);
+    }
+    return addr[dev];
+}
+
 struct DeviceBuffer {
     void *ptr = nullptr;
     ~DeviceBuffer() {
@@ -303,6 +405,60 @@ int64_t pi_filter_run(const uint8_t *cycle, int cycleLen, const uint8_t *triple,
     const int64_t kept = std::min<int64_t>((int64_t)hits, maxRows);
     if (kept > 0 && out &&
         !ok(cudaMemcpy(out, rows.ptr, (size_t)kept * (size_t)n, cudaMemcpyDeviceToHost), err, "read rows"))
+        return -3;
+    return (int64_t)hits;
+}
+
+int64_t pi_filter_noalloc_run(const uint8_t *cycle, int cycleLen, const uint8_t *triple, int tripleLen, int n,
+                              int skip2Move, uint8_t *outDevice, int64_t maxRows, cudaStream_t stream,
+                              std::string &err) {
+    if (n < 1 || n > kNoAllocMaxN) {
+        err = "tdp_pi_filter_noalloc: n must be in 1..12 (its static scratch covers (n-1)! <= 11! candidates); "
+              "use tdp_pi_filter for larger n";
+        return -1;
+    }
+    if (cycleLen < 0 || cycleLen > 63 || tripleLen < 0 || tripleLen > 63 || maxRows < 0 ||
+        (maxRows > 0 && !outDevice) || (cycleLen > 0 && !cycle) || (tripleLen > 0 && !triple)) {
+        err = "tdp_pi_filter_noalloc: invalid cycle/triple length, row limit or output buffer";
+        return -1;
+    }
+    for (int i = 0; i < cycleLen; ++i)
+        if (cycle[i] >= n) {
+            err = "tdp_pi_filter_noalloc: cycle symbol out of range";
+            return -1;
+        }
+    for (int i = 0; i < tripleLen; ++i)
+        if (triple[i] >= n) {
+            err = "tdp_pi_filter_noalloc: triple symbol out of range";
+            return -1;
+        }
+    unsigned long long *scratch = noalloc_scratch(err);
+    if (!scratch) return -3;
+    FilterArgs A;
+    std::memset(&A, 0, sizeof(A));
+    std::memcpy(A.cycle, cycle, cycleLen);
+    std::memcpy(A.triple, triple, tripleLen);
+    for (int i = 0; i < cycleLen; ++i) A.cycleIndex[cycle[i]] = (uint8_t)i;
+    A.fact[0] = 1;
+    for (int i = 1; i < 21; ++i) A.fact[i] = A.fact[i - 1] * (unsigned long long)i;
+    A.cycleLen = cycleLen;
+    A.tripleLen = tripleLen;
+    A.n = n;
+    A.skip2Move = skip2Move ? 1 : 0;
+    A.total = A.fact[n - 1 > 0 ? n - 1 : 0];
+    A.base = 0;
+    const int blocks = (int)((A.total + kRanksPerBlock - 1) / kRanksPerBlock);
+    // The scratch keeps the previous call's contents: the hit total starts at zero.
+    if (!ok(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), stream), err, "tdp_pi_filter_noalloc")) return -3;
+    noalloc_count_kernel<<<blocks, kThreads, 0, stream>>>(A, scratch, blocks);
+    noalloc_scan_kernel<<<1, kThreads, 0, stream>>>(scratch, blocks);
+    if (maxRows > 0)
+        noalloc_write_kernel<<<blocks, kThreads, 0, stream>>>(A, scratch, outDevice, (unsigned long long)maxRows);
+    if (!ok(cudaGetLastError(), err, "tdp_pi_filter_noalloc launch")) return -3;
+    unsigned long long hits = 0;
+    if (!ok(cudaMemcpyAsync(&hits, scratch, sizeof(hits), cudaMemcpyDeviceToHost, stream), err,
+            "tdp_pi_filter_noalloc read") ||
+        !ok(cudaStreamSynchronize(stream), err, "tdp_pi_filter_noalloc"))
         return -3;
     return (int64_t)hits;
 }
