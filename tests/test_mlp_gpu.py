@@ -75,7 +75,8 @@ def test_softmax_xent_matches_torch(native_lib, torch_cuda):
     import torch
     from tdp1375_b200 import order_model
     rows = 8
-    logits = torch.randn(rows, 5120, device="cuda")
+    g = torch.Generator(device="cpu").manual_seed(1375)
+    logits = torch.randn(rows, 5120, generator=g).cuda()
     ns = torch.tensor([32, 30, 24, 18, 12, 32, 9, 27], dtype=torch.uint8, device="cuda")
     valid = torch.zeros(rows, 4960, dtype=torch.bool)
     lex = order_model.LEX32
@@ -98,7 +99,8 @@ def test_softmax_xent_matches_torch(native_lib, torch_cuda):
     ref_loss = torch.nn.functional.cross_entropy(masked, target.long(), reduction="none")
     assert torch.allclose(loss, ref_loss, atol=1e-4, rtol=1e-4)
     ref_grad = (torch.softmax(masked, 1) - torch.nn.functional.one_hot(target.long(), 4960)) / rows
-    assert torch.allclose(dl[:, :4960].float(), ref_grad, atol=2e-4)
+    # dlogits is stored in bf16: 8 significant bits, so allow its relative rounding (2^-8)
+    assert torch.allclose(dl[:, :4960].float(), ref_grad, atol=1e-6, rtol=2 ** -8)
     assert float(dl[:, 4960:].float().abs().max()) == 0.0
 
 
