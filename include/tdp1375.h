@@ -130,6 +130,20 @@ int tdp_set_engine_config(int slot, const tdp_engine_config *cfg);
 
 int tdp_device_count(void);
 
+/* ---- batched extension filter (no counterpart in the reference) -----------------------
+ * Applies the permutation-filter predicates of tdp_pi_filter to every extension of `count`
+ * base configurations (spi/pi rows of 64 bytes, n symbols each, 3 <= n <= 60) that adds one
+ * 3-cycle: 2*C(n,3) extensions on existing symbols (spi o (a b c) and spi o (a c b)) followed
+ * by 2*C(n+3,3) on three new symbols n, n+1, n+2 inserted into pi before positions
+ * g1 <= g2 <= g3 (as (x y z) and (x z y)).  An extension is kept (keep byte 1) when its added
+ * cycle is in cyclic order in pi', some cycle is oriented and no oriented cycle admits a
+ * 2-move.  keep has count * tdp_extension_count(n) bytes; returns the number kept. */
+int tdp_extension_count(int n);
+int64_t tdp_extension_filter(const uint8_t *spi, const uint8_t *pi, int n, int count, uint8_t *keep);
+/* Same on device buffers, on `stream`; returns 0 (the caller counts keep bytes). */
+int tdp_extension_filter_device(const uint8_t *spi, const uint8_t *pi, int n, int count, uint8_t *keep,
+                                void *stream);
+
 /* ---- learned move ordering (no counterpart in the reference) ------------------------
  * A 1088 -> 256 -> 256 -> 256 -> 4960 BF16 MLP (fp32 accumulation on the tcgen05 tensor
  * cores) scores the (i,j,k) triples of a configuration with n <= 32; the batched search then

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/tdp1375.h"
+#include "extension_filter.h"
 #include "pi_filter.h"
 #include "search_engine.h"
 
@@ -358,4 +359,45 @@ extern "C" int64_t tdp_pi_filter_noalloc(const uint8_t *cycle, int cycle_len, co
                                                   out_device, max_rows, static_cast<cudaStream_t>(stream), err);
     if (rc >= 0) return rc;
     return fail(rc == -1 ? TDP_ERR_ARGUMENT : TDP_ERR_CUDA, err);
+}
+
+extern "C" int tdp_extension_count(int n) { return (n < 3 || n > 60) ? 0 : tdp::extension_count(n); }
+
+extern "C" int tdp_extension_filter_device(const uint8_t *spi, const uint8_t *pi, int n, int count, uint8_t *keep,
+                                           void *stream) {
+    std::string err;
+    const int rc = tdp::extension_filter_device(spi, pi, n, count, keep, static_cast<cudaStream_t>(stream), err);
+    if (rc != 0) return fail(rc == -1 ? TDP_ERR_ARGUMENT : TDP_ERR_CUDA, err);
+    return 0;
+}
+
+extern "C" int64_t tdp_extension_filter(const uint8_t *spi, const uint8_t *pi, int n, int count, uint8_t *keep) {
+    if (n < 3 || n > 60 || count < 0 || (count > 0 && (!spi || !pi || !keep)))
+        return fail(TDP_ERR_ARGUMENT, "tdp_extension_filter: n must be in 3..60 with non-null buffers");
+    if (count == 0) return 0;
+    const size_t per = (size_t)tdp::extension_count(n), rows = (size_t)count * 64, total = (size_t)count * per;
+    uint8_t *dSpi = nullptr, *dPi = nullptr, *dKeep = nullptr;
+    auto release = [&] {
+        cudaFree(dSpi);
+        cudaFree(dPi);
+        cudaFree(dKeep);
+    };
+    if (cudaMalloc(&dSpi, rows) != cudaSuccess || cudaMalloc(&dPi, rows) != cudaSuccess ||
+        cudaMalloc(&dKeep, total) != cudaSuccess) {
+        release();
+        return fail(TDP_ERR_OUT_OF_MEMORY, "tdp_extension_filter: device allocation failed");
+    }
+    std::string err;
+    int rc = 0;
+    if (cudaMemcpy(dSpi, spi, rows, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dPi, pi, rows, cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = -3, err = "tdp_extension_filter: upload failed";
+    if (rc == 0) rc = tdp::extension_filter_device(dSpi, dPi, n, count, dKeep, nullptr, err);
+    if (rc == 0 && cudaMemcpy(keep, dKeep, total, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = -3, err = "tdp_extension_filter: download failed";
+    release();
+    if (rc != 0) return fail(rc == -1 ? TDP_ERR_ARGUMENT : TDP_ERR_CUDA, err);
+    int64_t hits = 0;
+    for (size_t i = 0; i < total; ++i) hits += keep[i];
+    return hits;
 }

@@ -78,6 +78,9 @@ SIGNATURES = {
     "tdp_mlp_error": (ctypes.c_int, []),
     "tdp_set_order_model": (ctypes.c_int, [ctypes.c_int] + [vp] * 8),
     "tdp_enable_order_model": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "tdp_extension_count": (ctypes.c_int, [ctypes.c_int]),
+    "tdp_extension_filter": (ctypes.c_int64, [vp, vp, ctypes.c_int, ctypes.c_int, vp]),
+    "tdp_extension_filter_device": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]),
     "tdp_pi_filter_noalloc": (ctypes.c_int64, [u8p, ctypes.c_int, u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
                                                ctypes.c_int64, vp]),
 }
