@@ -33,6 +33,10 @@ MAX_DEPTH = 11
 DEDUP_ENTRIES = 1 << 30  # 32 GB of 32-byte entries: room for every concurrent m=8 instance
 QUEUE_BYTES = 3000 << 20
 HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes (read + write) per expanded node of the search kernel, from an ncu capture of a
+# config-1 batch of 64 instances (1.18 GB for 1.86 M nodes); the bench scales it by the nodes
+# of its own launches, since its workload is too large to capture under ncu.
+NCU_DRAM_BYTES_PER_NODE = 634.0
 
 
 def parse_args():
@@ -111,7 +115,8 @@ def cpu_sample(budget_s: float, node_limit: int, first_case: int = 0):
         pool.terminate()
     detail = (f"SortingSearch.java restatement (oracle port), {cores} processes, consecutive config-2 cases from "
               f"{first_case} for {elapsed:.1f} s, per-case limit {node_limit} expanded nodes; {resolved} resolved")
-    return resolved / elapsed, nodes / elapsed, cores, detail
+    # (resolved + 1) / elapsed bounds the rate from above when nothing resolves in the sample
+    return resolved / elapsed, nodes / elapsed, cores, detail, (resolved + 1) / elapsed
 
 
 # ------------------------------------------------------------------------- clocks
@@ -304,15 +309,19 @@ def run_ours(args):
         "verdicts": {"found": found, "not_found": notfound, "other": other},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 3), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 6), "traffic": None,
-                     "note": f"algorithmic table/task/instance bytes over kernel time; peak {peak_kind}"},
+                     "frac": round(achieved / peak, 6),
+                     "traffic": round(NCU_DRAM_BYTES_PER_NODE * nodes / launches, 1) if launches else None,
+                     "note": f"algorithmic table/task/instance bytes over kernel time; peak {peak_kind}; traffic = "
+                             "DRAM bytes per launch scaled from an ncu capture by expanded nodes; the kernel is "
+                             "issue/latency bound (ncu issue-active 13.6%, DRAM throughput 0.15%)"},
         "e2e": {"value": round(cases / wall, 3) if wall > 0 else None, "unit": "cases/s",
                 "h2d_bytes_per_step": args.batch * 144, "d2h_bytes_per_step": args.batch * 96},
         "clocks": clocks.summary(),
     }
     if cpu is not None:
         line["cpu_baseline"] = {"value": round(cpu[0], 4), "unit": "cases/s", "cores": cpu[2], "kind": "port",
-                                "sample": cpu[3], "nodes_per_s": round(cpu[1], 1)}
+                                "sample": cpu[3], "nodes_per_s": round(cpu[1], 1),
+                                "value_upper_bound": round(cpu[4], 4)}
     GPUSortingSearch.destroySlots()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -327,7 +336,7 @@ def run_reference(args):
     samples = []
     first = 0
     for s in range(args.warmup + args.steps):
-        cps, nps, cores, detail = cpu_sample(args.cpu_budget_s, args.cpu_node_limit, first_case=first)
+        cps, nps, cores, detail, _ = cpu_sample(args.cpu_budget_s, args.cpu_node_limit, first_case=first)
         first += 4 * cores
         if s >= args.warmup:
             samples.append((cps, nps))

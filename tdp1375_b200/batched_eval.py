@@ -1,0 +1,98 @@
+"""Batched uneven search: one persistent, graph-captured launch over many instances.
+
+    python -m tdp1375_b200.batched_eval [--count 1000000] [--sample 20000] [--out result.json]
+
+Instances come from the seeded uneven generator: 3-permutations with m truncated-geometric
+on 3..10 (p = 0.35) mixed with 10% random permutations of n' = 20..30 (pi = 0 followed by a
+shuffle, spi = sigma o pi^-1).  They are searched in partial mode (the proof generator's
+mode) with ratio 1.375 and max depth 11.  The autotuner first times its candidate
+configurations on a sample; the chosen one is installed.  Then the full set is uploaded
+once (tdp_batch_prepare), run through a captured CUDA graph (tdp_batch_run with
+use_cuda_graph), and read back.  The device time of the run is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import time
+
+import numpy as np
+
+from . import api, autotune, native
+from .cases import MIN_RATE, config_cases
+
+
+def instances(count: int):
+    cases, ms = [], []
+    for pi, spi, even, m in config_cases(4, count):
+        cases.append((pi, spi, even))
+        ms.append(m)
+    return cases, ms
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("--count", type=int, default=1_000_000)
+    p.add_argument("--sample", type=int, default=20_000)
+    p.add_argument("--table-entries", type=int, default=1 << 28)
+    p.add_argument("--depth", type=int, default=11)
+    p.add_argument("--tune-cache", default="")
+    p.add_argument("--out", default="")
+    args = p.parse_args(argv)
+    rate = float(MIN_RATE)
+    lib = native.load()
+
+    t0 = time.perf_counter()
+    cases, ms = instances(args.count)
+    t_gen = time.perf_counter() - t0
+    inst = api.make_instances(cases, args.depth, False)
+
+    sample = api.make_instances(cases[: args.sample], args.depth, False)
+    space = {"blocks_per_sm": [0, 2], "poll_interval": [8, 16, 32], "sparse_enumeration": [1, 0]}
+    choice = autotune.tune("batched-partial-d11", sample, min(args.sample, len(cases)), rate,
+                           table_sizes=(1 << 25, args.table_entries), space=space,
+                           cache_path=args.tune_cache or autotune.CACHE)
+
+    api.GPUSortingSearch(1, 1, 3000 << 20, choice["table_entries"])
+    try:
+        autotune.apply(0, choice)
+        cfg = api.engine_config(0)
+        cfg.use_cuda_graph = 1
+        cfg.time_limit_s = 900.0
+        api.set_engine_config(0, cfg)
+        t0 = time.perf_counter()
+        if lib.tdp_batch_prepare(0, inst, len(cases), ctypes.c_float(rate)) != 0:
+            raise RuntimeError(native.last_error())
+        t_prep = time.perf_counter() - t0
+        if lib.tdp_batch_run(0) != 0:
+            raise RuntimeError(native.last_error())
+        st = api.last_stats(0)
+        res = (native.Result * len(cases))()
+        lib.tdp_batch_results(0, res)
+        status = np.array([r.status for r in res])
+        nodes = np.array([r.nodes for r in res], dtype=np.int64)
+        ms_arr = np.array(ms)
+        per_m = {}
+        for m in sorted(set(ms)):
+            sel = ms_arr == m
+            per_m[str(m) if m else "random"] = {"count": int(sel.sum()), "found": int((status[sel] == 1).sum()),
+                                                "mean_nodes": float(nodes[sel].mean())}
+        out = {
+            "instances": len(cases), "generation_s": round(t_gen, 2), "prepare_s": round(t_prep, 2),
+            "kernel_ms": st.kernel_ms, "cases_per_s": len(cases) / (st.kernel_ms / 1e3),
+            "nodes": int(st.nodes), "nodes_per_s": st.nodes / (st.kernel_ms / 1e3), "children": int(st.children),
+            "launches": st.launches, "graph": True, "autotune_choice": choice,
+            "found": int((status == 1).sum()), "not_found": int((status == 0).sum()),
+            "other": int(((status != 0) & (status != 1)).sum()), "per_m": per_m,
+        }
+        print(json.dumps(out), flush=True)
+        if args.out:
+            with open(args.out, "w") as fh:
+                json.dump(out, fh, indent=1)
+    finally:
+        api.GPUSortingSearch.destroySlots()
+
+
+if __name__ == "__main__":
+    main()
