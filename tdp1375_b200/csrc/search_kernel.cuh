@@ -207,9 +207,16 @@ __device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t gene
     auto *table = reinterpret_cast<DedupEntry<KW> *>(P.table);
     const uint32_t base = (uint32_t)(h >> 24) & P.tableMask & ~7u;
     ++ls.probes;
+    // Eight independent relaxed tag loads (one round trip); only when a tag matches does the
+    // lane pay an acquire fence before reading keys, which pairs with the release store that
+    // published the entry.  (Eight acquire loads would serialise into eight round trips.)
     uint32_t tags[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) tags[q] = ld_acquire_u32(&table[base + q].tag);
+    for (int q = 0; q < 8; ++q) tags[q] = ld_relaxed_u32(&table[base + q].tag);
+    bool anyMatch = false;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) anyMatch |= (tags[q] == tag);
+    if (anyMatch) asm volatile("fence.acq_rel.gpu;" ::: "memory");
     unsigned freeMask = 0;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
