@@ -93,3 +93,21 @@ def config_cases(config: int, count: int, start: int = 0):
             raise ValueError(f"no generator for config {config}")
         pi, spi, even = three_permutation(m, rng)
         yield pi, spi, even, m
+
+
+def extension_bases(count: int, start: int = 0, m: int = 6):
+    """Base configurations of the extension enumeration: (pi, spi) rows of 64 bytes.
+
+    Each base is a product of m disjoint 3-cycles drawn uniformly over n = 3m symbols with pi
+    the identity array (seed ``seed_for(3, case)``).  Returns two (count, 64) uint8 arrays
+    and n.
+    """
+    n = 3 * m
+    spi = np.zeros((count, 64), np.uint8)
+    pi = np.zeros((count, 64), np.uint8)
+    for r, case in enumerate(range(start, start + count)):
+        rng = np.random.Generator(np.random.PCG64(seed_for(3, case)))
+        p, s, _ = three_permutation(m, rng)
+        spi[r, :n] = s
+        pi[r, :n] = p
+    return pi, spi, n

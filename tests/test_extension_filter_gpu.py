@@ -45,3 +45,22 @@ def test_extension_filter_matches_oracle(native_lib, oracle, unoriented):
     assert hits == want_total
     if unoriented:
         assert hits > count
+
+
+def test_extension_filter_seeded_bases_match_oracle(native_lib, oracle):
+    """The seeded m=6 bases of the extension workload: hit list and count bit-exact."""
+    from tdp1375_b200.cases import extension_bases
+    L = oracle.lib()
+    L.oracle_extension_filter.restype = ctypes.c_int64
+    count = 64
+    pi, spi, n = extension_bases(count)
+    per = native_lib.tdp_extension_count(n)
+    keep = np.zeros(count * per, np.uint8)
+    hits = native_lib.tdp_extension_filter(spi.ctypes.data_as(ctypes.c_void_p), pi.ctypes.data_as(ctypes.c_void_p),
+                                           n, count, keep.ctypes.data_as(ctypes.c_void_p))
+    want_total = 0
+    for b in range(count):
+        want = (ctypes.c_uint8 * per)()
+        want_total += L.oracle_extension_filter(oracle._u8(spi[b, :n]), oracle._u8(pi[b, :n]), n, want)
+        assert bytes(keep[b * per:(b + 1) * per]) == bytes(want), b
+    assert hits == want_total
