@@ -23,6 +23,10 @@ from . import api, autotune, native
 from .cases import MIN_RATE, config_cases
 
 
+WORKLOAD = "batched-partial-d11"
+STAT_FIELDS = ("nodes", "children", "dedup_probes", "dedup_pruned", "dedup_inserts", "dedup_full", "donations")
+
+
 def instances(count: int):
     cases, ms = [], []
     for pi, spi, even, m in config_cases(4, count):
@@ -38,6 +42,9 @@ def main(argv=None):
     p.add_argument("--table-entries", type=int, default=1 << 28)
     p.add_argument("--depth", type=int, default=11)
     p.add_argument("--tune-cache", default="")
+    p.add_argument("--run-table-entries", type=int, default=0, help="table for the full run (0: the tuned one)")
+    p.add_argument("--time-limit-s", type=float, default=600.0)
+    p.add_argument("--use-cached", action="store_true", help="reuse a cached autotune choice when present")
     p.add_argument("--out", default="")
     args = p.parse_args(argv)
     rate = float(MIN_RATE)
@@ -48,25 +55,33 @@ def main(argv=None):
     t_gen = time.perf_counter() - t0
     inst = api.make_instances(cases, args.depth, False)
 
-    sample = api.make_instances(cases[: args.sample], args.depth, False)
-    space = {"blocks_per_sm": [0, 2], "poll_interval": [8, 16, 32], "sparse_enumeration": [1, 0]}
-    choice = autotune.tune("batched-partial-d11", sample, min(args.sample, len(cases)), rate,
-                           table_sizes=(1 << 25, args.table_entries), space=space,
-                           cache_path=args.tune_cache or autotune.CACHE)
+    cache_path = args.tune_cache or autotune.CACHE
+    choice = autotune.cached(WORKLOAD, cache_path) if args.use_cached else None
+    if choice is None:
+        sample = api.make_instances(cases[: args.sample], args.depth, False)
+        space = {"blocks_per_sm": [0, 2], "poll_interval": [8, 16, 32], "sparse_enumeration": [1, 0]}
+        choice = autotune.tune(WORKLOAD, sample, min(args.sample, len(cases)), rate,
+                               table_sizes=(1 << 25, args.table_entries), space=space, cache_path=cache_path)
 
-    api.GPUSortingSearch(1, 1, 3000 << 20, choice["table_entries"])
+    print(json.dumps({"phase": "tuned", "generation_s": round(t_gen, 2), "choice": choice}), flush=True)
+    entries = args.run_table_entries or choice["table_entries"]
+    api.GPUSortingSearch(1, 1, 3000 << 20, entries)
     try:
         autotune.apply(0, choice)
         cfg = api.engine_config(0)
         cfg.use_cuda_graph = 1
-        cfg.time_limit_s = 900.0
+        cfg.time_limit_s = args.time_limit_s
         api.set_engine_config(0, cfg)
         t0 = time.perf_counter()
         if lib.tdp_batch_prepare(0, inst, len(cases), ctypes.c_float(rate)) != 0:
             raise RuntimeError(native.last_error())
         t_prep = time.perf_counter() - t0
         if lib.tdp_batch_run(0) != 0:
-            raise RuntimeError(native.last_error())
+            err = native.last_error()
+            st = api.last_stats(0)
+            print(json.dumps({"phase": "run failed", "error": err, "kernel_ms": st.kernel_ms,
+                              "stats": {f: int(getattr(st, f)) for f in STAT_FIELDS}}), flush=True)
+            raise RuntimeError(err)
         st = api.last_stats(0)
         res = (native.Result * len(cases))()
         lib.tdp_batch_results(0, res)
@@ -82,7 +97,8 @@ def main(argv=None):
             "instances": len(cases), "generation_s": round(t_gen, 2), "prepare_s": round(t_prep, 2),
             "kernel_ms": st.kernel_ms, "cases_per_s": len(cases) / (st.kernel_ms / 1e3),
             "nodes": int(st.nodes), "nodes_per_s": st.nodes / (st.kernel_ms / 1e3), "children": int(st.children),
-            "launches": st.launches, "graph": True, "autotune_choice": choice,
+            "launches": st.launches, "graph": True, "autotune_choice": choice, "table_entries": entries,
+            "stats": {f: int(getattr(st, f)) for f in STAT_FIELDS},
             "found": int((status == 1).sum()), "not_found": int((status == 0).sum()),
             "other": int(((status != 0) & (status != 1)).sum()), "per_m": per_m,
         }
