@@ -241,7 +241,8 @@ def run_ours(args):
             barrier()
             if s >= args.warmup:
                 kernel_ms.append(st.kernel_ms)
-                stats.append((st.nodes, st.children, st.dedup_probes, st.dedup_inserts, st.donations, st.launches))
+                stats.append((st.nodes, st.children, st.dedup_probes, st.dedup_inserts, st.donations, st.launches,
+                              st.busy_warp_cycles, st.warp_cycles))
                 res = (native.Result * args.batch)()
                 lib.tdp_batch_results(0, res)
                 for r in res:
@@ -307,6 +308,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{world} (cases sharded, no collective)"},
         "nodes_per_s": round(nodes / (sum(kernel_ms) / 1e3), 1),
         "verdicts": {"found": found, "not_found": notfound, "other": other},
+        "warp_busy_frac": round(sum(x[6] for x in stats) / max(1, sum(x[7] for x in stats)), 4),
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 3), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 6),

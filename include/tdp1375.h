@@ -110,6 +110,8 @@ typedef struct tdp_stats {
     double kernel_ms;
     int32_t error;
     int32_t launches;
+    uint64_t busy_warp_cycles; /* SM cycles warps spent holding a task, summed over warps */
+    uint64_t warp_cycles;      /* SM cycles from each warp's start to its exit, summed */
 } tdp_stats;
 
 /* Statistics of the last search/batch run on the slot. */

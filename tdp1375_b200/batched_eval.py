@@ -24,7 +24,8 @@ from .cases import MIN_RATE, config_cases
 
 
 WORKLOAD = "batched-partial-d11"
-STAT_FIELDS = ("nodes", "children", "dedup_probes", "dedup_pruned", "dedup_inserts", "dedup_full", "donations")
+STAT_FIELDS = ("nodes", "children", "dedup_probes", "dedup_pruned", "dedup_inserts", "dedup_full", "donations",
+               "busy_warp_cycles", "warp_cycles")
 
 
 def instances(count: int):

@@ -66,6 +66,8 @@ enum EngineStat : int {
     kStatDedupFull,
     kStatDonations,
     kStatTaskPops,
+    kStatBusyCycles,  // SM cycles warps spent holding a task
+    kStatWarpCycles,  // SM cycles of every warp from start to exit
     kStatCount
 };
 

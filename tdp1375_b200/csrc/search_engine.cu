@@ -563,6 +563,8 @@ tdp_stats SearchSlot::stats() const {
     s.dedup_full = statsAccum_[kStatDedupFull];
     s.donations = statsAccum_[kStatDonations];
     s.task_pops = statsAccum_[kStatTaskPops];
+    s.busy_warp_cycles = statsAccum_[kStatBusyCycles];
+    s.warp_cycles = statsAccum_[kStatWarpCycles];
     s.kernel_ms = kernelMs_;
     s.error = deviceError_;
     s.launches = launches_;

@@ -226,6 +226,13 @@ __device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t gene
             bool eq = true;
 #pragma unroll
             for (int kq = 0; kq < KW; ++kq) eq &= (__ldcg(&e->key[kq]) == key[kq]);
+            // Best depths only decrease, so a value read after the fence that is already
+            // <= depth decides the prune without an atomic.
+            const uint32_t seen = ld_relaxed_u32(&e->depth);
+            if (eq && seen <= depth) {
+                ++ls.pruned;
+                return false;
+            }
             if (eq) {
                 const uint32_t prev = atomicMin(&e->depth, depth);
                 if (prev <= depth) {
@@ -427,6 +434,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
     const uint32_t gw = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     bool registered = false;
     int backoff = 64;
+    // Busy and lifetime cycles accumulate in the warp's shared counters (start times are
+    // subtracted, end times added; unsigned arithmetic wraps back), so no register stays live.
+    if (lane == 0) S.stats[kStatWarpCycles] -= (unsigned long long)clock64();
     int idleRound = 0;
     bool stopAll = false;
 
@@ -478,6 +488,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         }
         backoff = 64;
         idleRound = 0;
+        if (lane == 0) S.stats[kStatBusyCycles] -= (unsigned long long)clock64();
 
         // ---------------------------------------------------------------- set up
         uint32_t inst;
@@ -883,11 +894,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
             S.stats[kStatChildren] += tChildren;
         }
         if (outcome == 2) {
+            if (lane == 0) S.stats[kStatBusyCycles] += (unsigned long long)clock64();
             stopAll = true;
             break;
         }
         // ---------------------------------------------------------------- finish task
         if (lane == 0) {
+            S.stats[kStatBusyCycles] += (unsigned long long)clock64();
             atomicAdd(&P.out[inst].nodes, tNodes);
             atomicAdd(&P.out[inst].children, tChildren);
             const int prev = atomicSub(&P.out[inst].outstanding, 1);
@@ -919,6 +932,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         atomicAdd(&ctl->stats[kStatDedupFull], full);
         atomicAdd(&ctl->stats[kStatDonations], S.stats[kStatDonations]);
         atomicAdd(&ctl->stats[kStatTaskPops], S.stats[kStatTaskPops]);
+        S.stats[kStatWarpCycles] += (unsigned long long)clock64();
+        atomicAdd(&ctl->stats[kStatBusyCycles], S.stats[kStatBusyCycles]);
+        atomicAdd(&ctl->stats[kStatWarpCycles], S.stats[kStatWarpCycles]);
     }
 }
 

@@ -30,7 +30,8 @@ class Stats(ctypes.Structure):
     _fields_ = [("nodes", ctypes.c_uint64), ("children", ctypes.c_uint64), ("dedup_probes", ctypes.c_uint64),
                 ("dedup_pruned", ctypes.c_uint64), ("dedup_inserts", ctypes.c_uint64), ("dedup_full", ctypes.c_uint64),
                 ("donations", ctypes.c_uint64), ("task_pops", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
-                ("error", ctypes.c_int32), ("launches", ctypes.c_int32)]
+                ("error", ctypes.c_int32), ("launches", ctypes.c_int32),
+                ("busy_warp_cycles", ctypes.c_uint64), ("warp_cycles", ctypes.c_uint64)]
 
 
 class EngineConfig(ctypes.Structure):

@@ -27,7 +27,7 @@ def test_struct_layouts():
     from tdp1375_b200 import native
     assert ctypes.sizeof(native.Instance) == 136
     assert ctypes.sizeof(native.Result) == 208
-    assert ctypes.sizeof(native.Stats) == 8 * 8 + 8 + 8
+    assert ctypes.sizeof(native.Stats) == 8 * 8 + 8 + 8 + 2 * 8
     assert ctypes.sizeof(native.EngineConfig) == 32
 
 
