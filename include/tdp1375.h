@@ -125,6 +125,10 @@ typedef struct tdp_engine_config {
     double time_limit_s;     /* device deadline per launch */
     int32_t sparse_enumeration; /* 1 = same-cycle pair enumeration where -2 children are useless */
     int32_t use_cuda_graph;     /* 1 = tdp_batch_run replays one captured CUDA graph per prepared batch */
+    int32_t warps_per_instance; /* 0 = admit instances while any warp is free; w > 0 = at most
+                                   (grid warps / w) instances in flight, the other warps join them
+                                   through work donation (bounds the live transposition-table load) */
+    int32_t reserved;
 } tdp_engine_config;
 
 int tdp_get_engine_config(int slot, tdp_engine_config *cfg);

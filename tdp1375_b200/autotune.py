@@ -5,6 +5,8 @@ The engine's tunables and what they stand for in the batched-search design:
                            (8 warps per block);
   * ``poll_interval``      chunks between a busy warp's looks at the idle-warp ring, i.e.
                            the granularity at which work is split off and donated;
+  * ``warps_per_instance`` grid warps per in-flight instance (0: no cap), i.e. how many
+                           instances hold live table entries at once;
   * ``table_entries``      transposition-table capacity, i.e. its load for the batch;
   * ``sparse_enumeration`` same-cycle pair enumeration on or off.
 
@@ -55,7 +57,7 @@ def candidates(space: Dict[str, List[int]]) -> Iterable[Dict[str, int]]:
 
 def apply(slot: int, choice: Dict[str, int]) -> None:
     cfg = api.engine_config(slot)
-    for key in ("blocks_per_sm", "poll_interval", "sparse_enumeration"):
+    for key in ("blocks_per_sm", "poll_interval", "sparse_enumeration", "warps_per_instance"):
         if key in choice:
             setattr(cfg, key, int(choice[key]))
     api.set_engine_config(slot, cfg)

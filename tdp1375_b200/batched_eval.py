@@ -6,7 +6,9 @@ Instances come from the seeded uneven generator: 3-permutations with m truncated
 on 3..10 (p = 0.35) mixed with 10% random permutations of n' = 20..30 (pi = 0 followed by a
 shuffle, spi = sigma o pi^-1).  They are searched in partial mode (the proof generator's
 mode) with ratio 1.375 and max depth 11.  The autotuner first times its candidate
-configurations on a sample; the chosen one is installed.  Then the full set is uploaded
+configurations (poll interval, warps per instance, table size) on a sample; the chosen one
+is installed, with the transposition table raised to --run-table-entries (2^31 entries,
+64 GB) for the full run.  Then the full set is uploaded
 once (tdp_batch_prepare), run through a captured CUDA graph (tdp_batch_run with
 use_cuda_graph), and read back.  The device time of the run is reported.
 """
@@ -40,10 +42,12 @@ def main(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--count", type=int, default=1_000_000)
     p.add_argument("--sample", type=int, default=20_000)
-    p.add_argument("--table-entries", type=int, default=1 << 28)
+    p.add_argument("--table-entries", type=int, default=1 << 30)
     p.add_argument("--depth", type=int, default=11)
     p.add_argument("--tune-cache", default="")
-    p.add_argument("--run-table-entries", type=int, default=0, help="table for the full run (0: the tuned one)")
+    p.add_argument("--run-table-entries", type=int, default=(1 << 31) - 1,
+                   help="table for the full run when larger than the tuned one (rounded up to a power of two; "
+                        "the C ABI takes an int)")
     p.add_argument("--time-limit-s", type=float, default=600.0)
     p.add_argument("--use-cached", action="store_true", help="reuse a cached autotune choice when present")
     p.add_argument("--out", default="")
@@ -58,14 +62,19 @@ def main(argv=None):
 
     cache_path = args.tune_cache or autotune.CACHE
     choice = autotune.cached(WORKLOAD, cache_path) if args.use_cached else None
+    if choice is not None and "warps_per_instance" not in choice:
+        choice = None  # cached before this tunable existed
     if choice is None:
         sample = api.make_instances(cases[: args.sample], args.depth, False)
-        space = {"blocks_per_sm": [0, 2], "poll_interval": [8, 16, 32], "sparse_enumeration": [1, 0]}
+        space = {"poll_interval": [16, 32, 64], "sparse_enumeration": [1], "warps_per_instance": [0, 2, 8]}
         choice = autotune.tune(WORKLOAD, sample, min(args.sample, len(cases)), rate,
-                               table_sizes=(1 << 25, args.table_entries), space=space, cache_path=cache_path)
+                               table_sizes=(1 << 28, args.table_entries), space=space, cache_path=cache_path)
 
     print(json.dumps({"phase": "tuned", "generation_s": round(t_gen, 2), "choice": choice}), flush=True)
-    entries = args.run_table_entries or choice["table_entries"]
+    # A sample cannot show the live-entry load of the full run (thousands of long instances
+    # in flight for minutes), so the full run takes the larger of the tuned table and
+    # --run-table-entries.
+    entries = max(choice["table_entries"], args.run_table_entries)
     api.GPUSortingSearch(1, 1, 3000 << 20, entries)
     try:
         autotune.apply(0, choice)
@@ -98,7 +107,7 @@ def main(argv=None):
             "instances": len(cases), "generation_s": round(t_gen, 2), "prepare_s": round(t_prep, 2),
             "kernel_ms": st.kernel_ms, "cases_per_s": len(cases) / (st.kernel_ms / 1e3),
             "nodes": int(st.nodes), "nodes_per_s": st.nodes / (st.kernel_ms / 1e3), "children": int(st.children),
-            "launches": st.launches, "graph": True, "autotune_choice": choice, "table_entries": entries,
+            "launches": st.launches, "graph": True, "autotune_choice": choice, "table_entries": 1 << (entries - 1).bit_length(),
             "stats": {f: int(getattr(st, f)) for f in STAT_FIELDS},
             "found": int((status == 1).sum()), "not_found": int((status == 0).sum()),
             "other": int(((status != 0) & (status != 1)).sum()), "per_m": per_m,

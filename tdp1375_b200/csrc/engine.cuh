@@ -135,6 +135,7 @@ struct EngineParams {
     int sparse;                      // same-cycle pair enumeration allowed (n <= 32)
     const uint16_t *order;           // per-instance root child order (learned), or null
     int orderStride;
+    int maxInFlight;                 // admitted-but-unfinished instance cap (0 = none)
 };
 
 }  // namespace tdp

@@ -36,8 +36,6 @@ struct ExtArgs {
     uint8_t *keep;
 };
 
-__device__ __forceinline__ int comb3(int n) { return n < 3 ? 0 : n * (n - 1) * (n - 2) / 6; }
-
 __device__ __forceinline__ void decode_triple(int t, int n, int &i, int &j, int &k) {
     i = 0;
     while (i < n - 3 && t >= (n - 1 - i) * (n - 2 - i) / 2) t -= (n - 1 - i) * (n - 2 - i) / 2, ++i;

@@ -111,14 +111,12 @@ __global__ void __launch_bounds__(128, 1)
     uint64_t *empty = full + STAGES;
     uint64_t *done = empty + STAGES;
     uint32_t *tmemSlot = reinterpret_cast<uint32_t *>(done + 1);
-    __shared__ int failed;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tileN = blockIdx.x, tileM = blockIdx.y;
     const int kTiles = (p.K + BK - 1) / BK;
 
     if (threadIdx.x == 0) {
-        failed = 0;
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(smem_u32(full + s), 1);
             mbar_init(smem_u32(empty + s), 1);
@@ -140,10 +138,8 @@ __global__ void __launch_bounds__(128, 1)
     if (warp == 0 && lane == 0) {
         for (int kt = 0; kt < kTiles; ++kt) {
             const int s = kt % STAGES, round = kt / STAGES;
-            if (round > 0 && !mbar_wait(smem_u32(empty + s), (uint32_t)((round - 1) & 1), p.error)) {
-                failed = 1;
-                break;
-            }
+            // a timed-out wait has set p.error; the later waits give up the same way
+            if (round > 0 && !mbar_wait(smem_u32(empty + s), (uint32_t)((round - 1) & 1), p.error)) break;
             const uint32_t a = smem_u32(smem + s * STAGE_BYTES);
             const uint32_t b = a + A_BYTES;
             mbar_expect_tx(smem_u32(full + s), STAGE_BYTES);
@@ -156,7 +152,6 @@ __global__ void __launch_bounds__(128, 1)
         for (int kt = 0; kt < kTiles && ok; ++kt) {
             const int s = kt % STAGES, round = kt / STAGES;
             if (!mbar_wait(smem_u32(full + s), (uint32_t)(round & 1), p.error)) {
-                failed = 1;
                 ok = false;
                 break;
             }

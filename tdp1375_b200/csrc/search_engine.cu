@@ -323,6 +323,9 @@ void SearchSlot::launchClass(int cls, int offset, int count) {
     blocksPerSM = std::max(1, blocksPerSM);
     // every warp of the grid needs a mailbox
     const int grid = std::min(numSMs_ * blocksPerSM, mailboxes_ / dev::kWarpsPerBlock);
+    P.maxInFlight = cfg_.warps_per_instance > 0
+                        ? std::max(1, grid * dev::kWarpsPerBlock / cfg_.warps_per_instance)
+                        : 0;
     if (cls == 0) {
         dev::search_engine_kernel<1><<<grid, threads, 0, stream_>>>(P);
     } else {

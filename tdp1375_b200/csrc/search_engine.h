@@ -43,7 +43,14 @@ public:
     int searchBatch(const tdp_instance *instances, int count, float minRate, tdp_result *results, std::string &err);
 
     tdp_stats stats() const;
-    tdp_engine_config &config() { return cfg_; }
+    const tdp_engine_config &config() const { return cfg_; }
+    // A new configuration invalidates a captured graph (its launch parameters change).
+    void setConfig(const tdp_engine_config &c) {
+        const int capacity = cfg_.task_capacity;
+        cfg_ = c;
+        cfg_.task_capacity = capacity;
+        graphValid_ = false;
+    }
     int stagedCount() const { return count_; }
 
     // Learned root ordering (n <= 32 instances of a batch).
@@ -92,7 +99,7 @@ private:
     std::vector<int> order_;
     int count_ = 0, countSmall_ = 0;
 
-    tdp_engine_config cfg_{0, 8, 1, 0, 120.0, 1, 0};
+    tdp_engine_config cfg_{0, 8, 1, 0, 120.0, 1, 0, 0, 0};
     unsigned long long statsAccum_[kStatCount] = {};
     double kernelMs_ = 0.0;
     int deviceError_ = 0;

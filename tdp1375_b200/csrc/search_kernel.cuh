@@ -460,7 +460,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                     if ((stopFlag | cancelFlag) || late) kind = -1;
                 }
                 if (kind == 0 && !registered) {
-                    if (ld_relaxed_s32(&ctl->nextInstance) < P.count) {
+                    // With a cap, a warp admits only while fewer than maxInFlight admitted
+                    // instances are unfinished (a racy check: the cap may be exceeded by the
+                    // few warps that pass it together); otherwise it registers as a helper.
+                    // The warp that finishes an instance is unregistered, so it admits the
+                    // next one: the cap cannot leave instances unadmitted.
+                    const int next = ld_relaxed_s32(&ctl->nextInstance);
+                    const bool room =
+                        P.maxInFlight <= 0 || next - ld_relaxed_s32(&ctl->doneCount) < P.maxInFlight;
+                    if (next < P.count && room) {
                         const int i = atomicAdd(&ctl->nextInstance, 1);
                         if (i < P.count) {
                             kind = 2;

@@ -37,7 +37,8 @@ class Stats(ctypes.Structure):
 class EngineConfig(ctypes.Structure):
     _fields_ = [("blocks_per_sm", ctypes.c_int32), ("poll_interval", ctypes.c_int32), ("tight_bound", ctypes.c_int32),
                 ("task_capacity", ctypes.c_int32), ("time_limit_s", ctypes.c_double),
-                ("sparse_enumeration", ctypes.c_int32), ("use_cuda_graph", ctypes.c_int32)]
+                ("sparse_enumeration", ctypes.c_int32), ("use_cuda_graph", ctypes.c_int32),
+                ("warps_per_instance", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 assert ctypes.sizeof(Instance) == 136 and ctypes.sizeof(Result) == 208

@@ -28,7 +28,7 @@ def test_struct_layouts():
     assert ctypes.sizeof(native.Instance) == 136
     assert ctypes.sizeof(native.Result) == 208
     assert ctypes.sizeof(native.Stats) == 8 * 8 + 8 + 8 + 2 * 8
-    assert ctypes.sizeof(native.EngineConfig) == 32
+    assert ctypes.sizeof(native.EngineConfig) == 40
 
 
 def test_errors_without_slots(native_lib):
