@@ -123,7 +123,8 @@ typedef struct tdp_engine_config {
     int32_t tight_bound;     /* 1 = verdict-preserving strengthened prune, 0 = reference prune only */
     int32_t task_capacity;   /* read-only: warp mailboxes for work donation (sized from the queue budget) */
     double time_limit_s;     /* device deadline per launch */
-    int32_t sparse_enumeration; /* 1 = same-cycle pair enumeration where -2 children are useless */
+    int32_t sparse_enumeration; /* 0 = every (i,j,k); 1 = same-cycle pairs where -2 children are useless;
+                                   2 (default) = also same-cycle triples where only +2 children are useful */
     int32_t use_cuda_graph;     /* 1 = tdp_batch_run replays one captured CUDA graph per prepared batch */
     int32_t warps_per_instance; /* 0 = admit instances while any warp is free; w > 0 = at most
                                    (grid warps / w) instances in flight, the other warps join them

@@ -8,7 +8,8 @@ The engine's tunables and what they stand for in the batched-search design:
   * ``warps_per_instance`` grid warps per in-flight instance (0: no cap), i.e. how many
                            instances hold live table entries at once;
   * ``table_entries``      transposition-table capacity, i.e. its load for the batch;
-  * ``sparse_enumeration`` same-cycle pair enumeration on or off.
+  * ``sparse_enumeration`` 0 every triple, 1 same-cycle pairs, 2 pairs and same-cycle
+                           triples.
 
 ``tune`` times every candidate on a sample of the workload (engine kernel time from
 ``tdp_last_stats``; verdicts must agree across candidates), keeps the fastest, and caches
@@ -30,7 +31,7 @@ CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotune_cache
 DEFAULT_SPACE = {
     "blocks_per_sm": [0, 2, 1],
     "poll_interval": [4, 8, 16, 32],
-    "sparse_enumeration": [1, 0],
+    "sparse_enumeration": [2, 1],
 }
 
 

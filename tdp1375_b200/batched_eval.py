@@ -66,7 +66,7 @@ def main(argv=None):
         choice = None  # cached before this tunable existed
     if choice is None:
         sample = api.make_instances(cases[: args.sample], args.depth, False)
-        space = {"poll_interval": [16, 32, 64], "sparse_enumeration": [1], "warps_per_instance": [0, 2, 8]}
+        space = {"poll_interval": [16, 32, 64], "sparse_enumeration": [2], "warps_per_instance": [0, 2, 8]}
         choice = autotune.tune(WORKLOAD, sample, min(args.sample, len(cases)), rate,
                                table_sizes=(1 << 28, args.table_entries), space=space, cache_path=cache_path)
 

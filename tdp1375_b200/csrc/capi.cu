@@ -207,7 +207,7 @@ int tdp_set_engine_config(int slot, const tdp_engine_config *cfg) {
     auto s = get_slot(slot);
     if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
     if (!cfg || cfg->poll_interval <= 0 || cfg->time_limit_s <= 0 || cfg->blocks_per_sm < 0 ||
-        cfg->warps_per_instance < 0)
+        cfg->warps_per_instance < 0 || cfg->sparse_enumeration < 0 || cfg->sparse_enumeration > 2)
         return fail(TDP_ERR_ARGUMENT, "tdp_set_engine_config: invalid configuration");
     s->setConfig(*cfg);
     return 0;

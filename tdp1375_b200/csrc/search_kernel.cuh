@@ -336,20 +336,31 @@ __device__ __forceinline__ void apply_move(const uint32_t (&w)[NW], uint32_t (&o
     }
 }
 
-// Same-cycle pair enumeration.  When a frame's children can neither succeed nor be
-// admitted with a -2 change, and either 0-changes are useless too or the node has at most
-// one even-length cycle, every child worth evaluating has two of its three symbols in one
-// spi-cycle (a triple over three distinct cycles changes the odd-cycle count by -2, or by 0
-// only when two of the cycles have even length).  Such a frame enumerates pairs of
-// positions p < q whose symbols share a cycle, one pair per chunk, with the lane as the
-// third position r; a triple lying in one cycle is taken only from its two smallest
-// positions.  Only for n <= 32 (one position per lane).
+// Restricted child enumerations (n <= 32, one position per lane).  Both rest on the cycle
+// structure of spi: a child's odd-cycle count changes by +2 only if its three symbols lie
+// in one cycle, or two lie in one even-length cycle and the third in another even-length
+// cycle; a triple over three distinct cycles changes the count by -2, or by 0 only when two
+// of those cycles have even length.
+//
+// * Pairs (mode 1).  When no child with a -2 change is useful, and either 0-changes are
+//   useless too or the node has at most one even-length cycle, every useful child has two
+//   of its three symbols in one cycle.  The frame enumerates position pairs p < q whose
+//   symbols share a cycle, one pair per chunk, with the lane as the third position r; a
+//   triple lying in one cycle is taken only from its two smallest positions.
+// * Triples (mode 2).  When only +2 children are useful and the node has at most one
+//   even-length cycle, every useful child takes its three symbols from one cycle.  The
+//   frame enumerates the position triples p < q < r inside each cycle, 32 per chunk, from
+//   a list the warp writes to shared memory at frame set-up (at most kMaxTriples entries;
+//   a larger frame uses pairs).  In searches at the ratio limit this is nearly every frame,
+//   and a frame then needs one or two chunks instead of one per same-cycle pair.
+constexpr int kMaxTriples = 256;
+
 struct SparseFrame {
     uint32_t same;       // positions > lane whose symbol shares the cycle of pi[lane]
-    uint32_t incl;       // inclusive prefix of popc(same) over lanes
+    uint32_t incl;       // inclusive prefix over lanes of popc(same) (pairs) or C(popc(same), 2) (triples)
     uint32_t leaderPos;  // cycle leader of pi[lane]
-    int np;              // number of pairs
-    bool on;
+    int np;              // number of pairs or triples
+    int mode;            // 0 dense, 1 pairs, 2 triples
 };
 
 struct PairSel {
@@ -357,19 +368,23 @@ struct PairSel {
     uint32_t leader;
 };
 
+// allow: 0 dense only, 1 pairs, 2 pairs and triples.  triList (or null) receives the
+// triple list of a triple-mode frame; pass null to classify a frame without touching the
+// list of the frame being enumerated.
 template <int NW>
 __device__ __forceinline__ SparseFrame sparse_setup(const uint32_t (&w)[NW], int n, int lane, int even,
-                                                    uint64_t satMask, uint64_t expMask, int enable) {
+                                                    uint64_t satMask, uint64_t expMask, int allow,
+                                                    uint32_t *triList) {
     SparseFrame sf;
     sf.same = 0u;
     sf.incl = 0u;
     sf.leaderPos = 0u;
     sf.np = 0;
-    sf.on = false;
+    sf.mode = 0;
     if constexpr (NW != 1) {
         return sf;
     } else {
-        if (!enable) return sf;
+        if (allow <= 0) return sf;
         const uint64_t useful = satMask | expMask;
         const bool neg = even >= 2 && ((useful >> (even - 2)) & 1ull);
         if (neg) return sf;
@@ -380,17 +395,50 @@ __device__ __forceinline__ SparseFrame sparse_setup(const uint32_t (&w)[NW], int
         const uint32_t leaderPos = w_leader(gather<1>(w, w_pi(w[0])));
         const uint32_t key = (lane < n) ? leaderPos : 64u + (uint32_t)lane;
         const uint32_t same = __match_any_sync(kFull, key) & ~((2u << lane) - 1u);
-        uint32_t incl = (uint32_t)__popc(same);
+        sf.same = same;
+        sf.leaderPos = leaderPos;
+        const uint32_t k = (uint32_t)__popc(same);
+        if (allow >= 2 && !zero && evenLen <= 1) {
+            const uint32_t c2 = k * (k - 1u) / 2u;
+            uint32_t incl = c2;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int total = (int)__shfl_sync(kFull, incl, 31);
+            if (total <= kMaxTriples) {
+                if (triList) {
+                    __syncwarp();  // every lane is done reading the previous frame's list
+                    uint32_t at = incl - c2;
+                    uint32_t m1 = same;
+                    while (m1) {
+                        const uint32_t q = (uint32_t)(__ffs(m1) - 1);
+                        m1 &= m1 - 1u;
+                        uint32_t m2 = m1;
+                        while (m2) {
+                            const uint32_t r = (uint32_t)(__ffs(m2) - 1);
+                            m2 &= m2 - 1u;
+                            triList[at++] = pack_triple((uint32_t)lane, q, r);
+                        }
+                    }
+                    __syncwarp();
+                }
+                sf.incl = incl;
+                sf.np = total;
+                sf.mode = 2;
+                return sf;
+            }
+        }
+        uint32_t incl = k;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(kFull, incl, o);
             if (lane >= o) incl += y;
         }
-        sf.same = same;
         sf.incl = incl;
-        sf.leaderPos = leaderPos;
         sf.np = (int)__shfl_sync(kFull, incl, 31);
-        sf.on = true;
+        sf.mode = 1;
         return sf;
     }
 }
@@ -410,9 +458,34 @@ __device__ __forceinline__ PairSel sparse_pair(const SparseFrame &sf, int u) {
     return ps;
 }
 
+// Triple index u (uniform) of a triple-mode frame, decoded without its list, in list order:
+// owner position p, then the v-th pair q < r of the positions in same(p) (lexicographic).
+__device__ __forceinline__ uint32_t triple_at(const SparseFrame &sf, int u) {
+    const unsigned owner = __ballot_sync(kFull, sf.incl > (uint32_t)u);
+    const int p = __ffs(owner) - 1;
+    const uint32_t sameP = __shfl_sync(kFull, sf.same, p);
+    const uint32_t k = (uint32_t)__popc(sameP);
+    uint32_t v = (uint32_t)u - (__shfl_sync(kFull, sf.incl, p) - k * (k - 1u) / 2u);
+    uint32_t m1 = sameP, q = 0u, r = 0u;
+    for (uint32_t it = 0; it < 32u && m1; ++it) {
+        q = (uint32_t)(__ffs(m1) - 1);
+        m1 &= m1 - 1u;
+        const uint32_t cnt = (uint32_t)__popc(m1);
+        if (v < cnt) {
+            uint32_t m2 = m1;
+            for (uint32_t t = v; t > 0u; --t) m2 &= m2 - 1u;
+            r = (uint32_t)(__ffs(m2) - 1);
+            break;
+        }
+        v -= cnt;
+    }
+    return pack_triple((uint32_t)p, q, r);
+}
+
 template <int NW>
 struct WarpShared {
     uint32_t words[kMaxDepth + 1][NW * 32];
+    uint32_t tri[NW == 1 ? kMaxTriples : 1];  // triple list of the frame being enumerated
     uint32_t staging[52];
     unsigned long long stats[kStatCount];  // per-warp counters, flushed once at exit
 };
@@ -576,10 +649,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         // The root of an instance with a learned order enumerates its children in that order
         // (dense mode, index space = positions in the order).
         const uint16_t *rootOrder = (P.order && NW == 1) ? P.order + (size_t)inst * (size_t)P.orderStride : nullptr;
-        SparseFrame sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse && !(rootOrder && f == 0));
+        SparseFrame sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, (rootOrder && f == 0) ? 0 : P.sparse, S.tri);
         // A donated range is in the units of its frame's mode (the receiver derives the same
         // mode from the same node); hi = 0xFFFF covers every child.
-        if (hi == 0xFFFF) end = sf.on ? sf.np : T;
+        if (hi == 0xFFFF) end = sf.mode ? sf.np : T;
 
         // outcome: 0 subtree exhausted, 1 instance found (here or elsewhere), 2 launch stop
         int outcome = 0;
@@ -605,7 +678,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                     for (int h = 0; h < NW; ++h) w[h] = S.words[f][h * 32 + lane];
                     satMask = shfl64(ruleReg, f + 1);
                     expMask = shfl64(ruleReg, 16 + f + 1);
-                    sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse && !(rootOrder && f == 0));
+                    sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, (rootOrder && f == 0) ? 0 : P.sparse,
+                                          S.tri);
                     continue;
                 }
                 if (++poll >= P.pollInterval) {
@@ -641,7 +715,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                         // Candidates: the shallowest frame with >= 2 unevaluated chunks
                         // (split its range), or a shallower frame holding admitted children
                         // not yet descended into (hand over one of them as a fresh node).
-                        const int step = sf.on ? 1 : 32;
+                        const int step = sf.mode == 1 ? 1 : 32;
                         int remChunks = 0;
                         uint32_t pend = 0u;
                         if (lane >= baseDepth && lane < f) {
@@ -686,13 +760,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                                 const uint64_t gSat = shfl64(ruleReg, g + 1);
                                 const uint64_t gExp = shfl64(ruleReg, 16 + g + 1);
                                 const SparseFrame gsf =
-                                    sparse_setup<NW>(wg, n, lane, gEven, gSat, gExp, P.sparse && !(rootOrder && g == 0));
+                                    sparse_setup<NW>(wg, n, lane, gEven, gSat, gExp, (rootOrder && g == 0) ? 0 : P.sparse,
+                                                     nullptr);
                                 uint32_t ctr;
-                                if (gsf.on) {
+                                if (gsf.mode == 1) {
                                     const PairSel ps = sparse_pair(gsf, gChunk);
                                     ctr = (l < ps.p) ? pack_triple(l, ps.p, ps.q)
                                                      : (l < ps.q) ? pack_triple(ps.p, l, ps.q)
                                                                   : pack_triple(ps.p, ps.q, l);
+                                } else if (gsf.mode == 2) {
+                                    ctr = triple_at(gsf, gChunk + l);
                                 } else {
                                     const int t = gChunk + l;
                                     ctr = __ldg(trip + ((rootOrder && g == 0) ? (int)__ldg(rootOrder + t) : t));
@@ -777,7 +854,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                 bool valid;
                 int nValid;
                 chunk = cursor;
-                if (sf.on) {
+                if (sf.mode == 1) {
                     // one same-cycle position pair (p, q) per chunk, lane = third position r
                     cursor += 1;
                     const PairSel ps = sparse_pair(sf, chunk);
@@ -800,10 +877,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                     if (!valid) tr = a = b = c = 0u;
                     nValid = __popc(__ballot_sync(kFull, valid));
                 } else {
+                    // 32 consecutive triples: from the frame's same-cycle list (mode 2) or the
+                    // lexicographic table (mode 0, in learned order at a root that has one)
                     const int t = cursor + lane;
                     cursor += 32;
                     valid = t < end;
-                    tr = valid ? __ldg(trip + ((rootOrder && f == 0) ? (int)__ldg(rootOrder + t) : t)) : 0u;
+                    if (sf.mode == 2) {
+                        tr = valid ? S.tri[t] : 0u;
+                    } else {
+                        tr = valid ? __ldg(trip + ((rootOrder && f == 0) ? (int)__ldg(rootOrder + t) : t)) : 0u;
+                    }
                     a = w_pi(gather<NW>(w, tri_i(tr)));
                     b = w_pi(gather<NW>(w, tri_j(tr)));
                     c = w_pi(gather<NW>(w, tri_k(tr)));
@@ -850,11 +933,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
             const int l = __ffs(pending) - 1;
             pending &= pending - 1u;
             uint32_t tr;
-            if (sf.on) {
+            if (sf.mode == 1) {
                 const PairSel ps = sparse_pair(sf, chunk);
                 const int r = l;
                 tr = (r < ps.p) ? pack_triple(r, ps.p, ps.q)
                                 : (r < ps.q) ? pack_triple(ps.p, r, ps.q) : pack_triple(ps.p, ps.q, r);
+            } else if (sf.mode == 2) {
+                tr = S.tri[chunk + l];
             } else {
                 const int t = chunk + l;
                 tr = __ldg(trip + ((rootOrder && f == 0) ? (int)__ldg(rootOrder + t) : t));
@@ -865,7 +950,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                 fPending = pending;
                 fChunk = chunk;
                 fEven = even;
-                fStep = sf.on ? 1 : 32;
+                fStep = sf.mode == 1 ? 1 : 32;
                 fMove = tr;
 #pragma unroll
                 for (int q = 0; q < KW; ++q) fKey[q] = key[q];
@@ -891,9 +976,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
             for (int h = 0; h < NW; ++h) S.words[f][h * 32 + lane] = w[h];
             satMask = shfl64(ruleReg, f + 1);
             expMask = shfl64(ruleReg, 16 + f + 1);
-            sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, P.sparse && !(rootOrder && f == 0));
+            sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, (rootOrder && f == 0) ? 0 : P.sparse, S.tri);
             cursor = 0;
-            end = sf.on ? sf.np : T;
+            end = sf.mode ? sf.np : T;
             pending = 0u;
             ++tNodes;
         }

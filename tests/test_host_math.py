@@ -23,6 +23,18 @@ def test_move_delta_matches_recount(math_check):
     assert out.returncode == 0, out.stdout + out.stderr
 
 
+def test_enumeration_restrictions_hold(math_check):
+    """Same-cycle pairs (no -2 child useful) and same-cycle triples (only +2 useful, at most
+    one even-length cycle) cover every useful child."""
+    out = subprocess.run([math_check, "restrict"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+
+
+def test_triple_list_and_decoder(math_check):
+    out = subprocess.run([math_check, "triples"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+
+
 def test_tight_bound_is_sound(math_check):
     out = subprocess.run([math_check, "tight"], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr

@@ -75,16 +75,17 @@ def test_config1_verdicts_match_oracle(gpu_searcher, oracle):
 
 @pytest.mark.parametrize("full,depth", [(False, 8), (True, 8)])
 def test_engine_modes_keep_verdicts(gpu_searcher, oracle, full, depth):
-    """Single-instance calls, batched calls, and the engine with the tight bound and/or
-    the same-cycle pair enumeration switched off, or with instances in flight capped (64
-    warps per instance; a cap of one instance), all give the same verdicts."""
+    """Single-instance calls, batched calls, and the engine with the tight bound off, with
+    every triple enumerated, with same-cycle pairs only, with pairs and same-cycle triples,
+    or with instances in flight capped (64 warps per instance; a cap of one instance), all
+    give the same verdicts."""
     from tdp1375_b200 import GPUSortingSearch, api, native
     from tdp1375_b200.cases import config_cases
     cases = [c[:3] for c in config_cases(1, 40)]
     batch = run_batch(cases, depth, full, R1375)
     cfg = api.engine_config(1)
     variants = []
-    for tight, sparse, wpi in ((1, 0, 0), (0, 0, 0), (0, 1, 0), (1, 1, 64), (1, 1, 100000)):
+    for tight, sparse, wpi in ((1, 0, 0), (0, 0, 0), (0, 1, 0), (1, 1, 0), (0, 2, 0), (1, 2, 64), (1, 2, 100000)):
         api.set_engine_config(1, native.EngineConfig(cfg.blocks_per_sm, cfg.poll_interval, tight, cfg.task_capacity,
                                                      cfg.time_limit_s, sparse, 0, wpi))
         try:
