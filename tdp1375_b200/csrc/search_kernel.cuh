@@ -268,8 +268,7 @@ __device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t gene
             e->depth = depth;
 #pragma unroll
             for (int kq = 0; kq < KW; ++kq) __stcg(&e->key[kq], key[kq]);
-            __threadfence();
-            st_release_u32(&e->tag, tag);
+            st_release_u32(&e->tag, tag);  // the release orders the depth and key stores before it
             ++ls.inserts;
         }
     } else {
@@ -670,6 +669,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                     cursor = __shfl_sync(kFull, fCursor, f);
                     end = __shfl_sync(kFull, fEnd, f);
                     pending = __shfl_sync(kFull, fPending, f);
+                    // An exhausted parent is left at once: its words, key and enumeration
+                    // state are not needed.
+                    if (pending == 0u && cursor >= end) continue;
                     chunk = __shfl_sync(kFull, fChunk, f);
                     even = __shfl_sync(kFull, fEven, f);
 #pragma unroll
@@ -962,15 +964,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
             const uint32_t wa = gather<NW>(w, a);
             const uint32_t wb = gather<NW>(w, b);
             const uint32_t wc = gather<NW>(w, c);
-            even += move_delta(wa, wb, wc);
+            const int delta = move_delta(wa, wb, wc);
+            even += delta;
             set_field<NW>(key, a, w_spi(wc));
             set_field<NW>(key, b, w_spi(wa));
             set_field<NW>(key, c, w_spi(wb));
             uint32_t nw[NW];
             apply_move<NW>(w, nw, lane, i, j, k, a, b, c, wa, wb, wc);
+            // A +2 move with a, b, c in one cycle splits it into three arcs: the cycle fields
+            // follow per lane from a, b and c (no shuffles); other moves rebuild them.
+            const bool split = delta == 2 && w_leader(wa) == w_leader(wb) && w_leader(wb) == w_leader(wc);
 #pragma unroll
-            for (int h = 0; h < NW; ++h) w[h] = nw[h];
-            build_tables<NW>(w, n, lane);
+            for (int h = 0; h < NW; ++h) {
+                const int x = lane + 32 * h;
+                if (split && x < n) nw[h] |= split_cycle_fields(w[h], a, b, c, wa, wb, wc) & ~0xFFFu;
+                w[h] = nw[h];
+            }
+            if (!split) build_tables<NW>(w, n, lane);
             ++f;
 #pragma unroll
             for (int h = 0; h < NW; ++h) S.words[f][h * 32 + lane] = w[h];

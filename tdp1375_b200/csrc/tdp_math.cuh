@@ -25,7 +25,9 @@ constexpr int kMaxDepth = 15;  // MAX_DEPTH of the reference (core/common.cuh:29
 // keeps one 32-bit word for it:
 //   bits  0..5   spi[x]          image of symbol x under spi
 //   bits  6..11  pi[x]           symbol written at position x of the pi array
-//   bits 12..17  leader(x)       smallest symbol of x's spi-cycle
+//   bits 12..17  leader(x)       anchor of x's spi-cycle: its smallest symbol after a full
+//                                rebuild, the cycle's last moved symbol after a split
+//                                (split_cycle_fields); any one symbol per cycle works
 //   bits 18..23  s2l(x)          steps from x to its leader following spi
 //   bits 24..30  len(x)          length of x's spi-cycle
 // ---------------------------------------------------------------------------
@@ -76,6 +78,34 @@ TDP_HD int move_delta(uint32_t wa, uint32_t wb, uint32_t wc) {
         return ((Lb + dac) & 1) + ((La - dac) & 1) - (La & 1) - (Lb & 1);
     }
     return ((La + Lb + Lc) & 1) - (La & 1) - (Lb & 1) - (Lc & 1);
+}
+
+// Cycle fields of symbol x after the move (a b c) when a, b and c lie in one cycle in the
+// spi-order a -> b -> c (the split case of move_delta, a +2 change): the cycle breaks into
+// the arcs (a, b], (b, c] and (c, a], each anchored at its last element (b, c and a), with
+// steps counted forward to the anchor.  wx is x's word before the move; its spi/pi fields
+// are kept and words of other cycles are returned unchanged.  This replaces a full
+// pointer-jumping rebuild of the cycle fields after such a move.
+TDP_HD uint32_t split_cycle_fields(uint32_t wx, uint32_t a, uint32_t b, uint32_t c, uint32_t wa, uint32_t wb,
+                                   uint32_t wc) {
+    if (w_leader(wx) != w_leader(wa)) return wx;
+    const int L = (int)w_len(wa);
+    const int sa = (int)w_s2l(wa);
+    int dB = sa - (int)w_s2l(wb);  // forward distance a -> b
+    if (dB < 0) dB += L;
+    int dC = sa - (int)w_s2l(wc);  // a -> c
+    if (dC < 0) dC += L;
+    int dx = sa - (int)w_s2l(wx);  // a -> x
+    if (dx < 0) dx += L;
+    uint32_t anchor, steps, len;
+    if (dx >= 1 && dx <= dB) {
+        anchor = b, len = (uint32_t)dB, steps = (uint32_t)(dB - dx);
+    } else if (dx > dB && dx <= dC) {
+        anchor = c, len = (uint32_t)(dC - dB), steps = (uint32_t)(dC - dx);
+    } else {
+        anchor = a, len = (uint32_t)(L - dC), steps = dx == 0 ? 0u : (uint32_t)(L - dx);
+    }
+    return (wx & 0xFFFu) | (anchor << 12) | (steps << 18) | (len << 24);
 }
 
 // Block swap of [i,j) and [j,k) as a gather index (transposition.cuh:5-11).

@@ -6,7 +6,8 @@
 //  3. the tight bound never removes a state from which a success is reachable
 //     (brute force over small n by exhaustive search of gains);
 //  4. the child restrictions behind the pair and triple enumerations ("restrict");
-//  5. the triple list and its uniform decoder, emulated lane by lane ("triples").
+//  5. the triple list and its uniform decoder, emulated lane by lane ("triples");
+//  6. the incremental cycle fields after a split move ("split").
 #include <cstdio>
 #include <cstdlib>
 #include <random>
@@ -141,6 +142,80 @@ int main(int argc, char **argv) {
             check_spi(spi, n);
         }
         printf("restrict checked=%ld bad=%ld\n", checked, bad);
+        return bad == 0 ? 0 : 1;
+    }
+    if (std::string(mode) == "split") {
+        // split_cycle_fields against a recount: for random spi, chains of up to 6 split moves
+        // (a, b, c in one cycle, spi-order a -> b -> c) are applied with the incremental
+        // fields; after each, every symbol's anchor must lie in its child cycle, be reached
+        // in s2l steps (anchor: 0 steps), len must be the child cycle's length, and
+        // move_delta on the new words must equal a recount for random moves.
+        std::mt19937 rng(23);
+        long bad = 0, total = 0;
+        for (int it = 0; it < 4000; ++it) {
+            const int n = 3 + (int)(rng() % 30);
+            int spi[64];
+            uint32_t w[64];
+            for (int i = 0; i < n; ++i) spi[i] = i;
+            std::shuffle(spi, spi + n, rng);
+            for (int x = 0; x < n; ++x) {
+                int leader = x, cur = spi[x], len = 1;
+                while (cur != x) {
+                    leader = std::min(leader, cur);
+                    cur = spi[cur];
+                    ++len;
+                }
+                int steps = 0;
+                for (cur = x; cur != leader; cur = spi[cur]) ++steps;
+                w[x] = w_make(spi[x], 0, leader, steps, len);
+            }
+            for (int chain = 0; chain < 6; ++chain) {
+                int a = -1, b = -1, c = -1;
+                for (int tries = 0; tries < 200 && a < 0; ++tries) {
+                    const int x = rng() % n, y = rng() % n, z = rng() % n;
+                    if (x == y || y == z || x == z) continue;
+                    if (w_leader(w[x]) != w_leader(w[y]) || w_leader(w[y]) != w_leader(w[z])) continue;
+                    if (move_delta(w[x], w[y], w[z]) != 2) continue;
+                    a = x, b = y, c = z;
+                }
+                if (a < 0) break;
+                const uint32_t wa = w[a], wb = w[b], wc = w[c];
+                int child[64];
+                std::copy(spi, spi + n, child);
+                child[a] = spi[c];
+                child[b] = spi[a];
+                child[c] = spi[b];
+                uint32_t nw[64];
+                for (int x = 0; x < n; ++x)
+                    nw[x] = (split_cycle_fields(w[x], a, b, c, wa, wb, wc) & ~63u) | (uint32_t)child[x];
+                for (int x = 0; x < n; ++x) {
+                    ++total;
+                    int L = 1;
+                    for (int cur = child[x]; cur != x; cur = child[cur]) ++L;
+                    int cur = x;
+                    for (uint32_t s2 = 0; s2 < w_s2l(nw[x]); ++s2) cur = child[cur];
+                    const int anchor = (int)w_leader(nw[x]);
+                    if (cur != anchor || (int)w_len(nw[x]) != L || w_s2l(nw[anchor]) != 0 ||
+                        (int)w_leader(nw[anchor]) != anchor)
+                        ++bad;
+                }
+                std::copy(child, child + n, spi);
+                std::copy(nw, nw + n, w);
+                const int e0 = count_even(spi, n);
+                for (int q = 0; q < 30; ++q) {
+                    const int x = rng() % n, y = rng() % n, z = rng() % n;
+                    if (x == y || y == z || x == z) continue;
+                    int g[64];
+                    std::copy(spi, spi + n, g);
+                    g[x] = spi[z];
+                    g[y] = spi[x];
+                    g[z] = spi[y];
+                    ++total;
+                    if (count_even(g, n) - e0 != move_delta(w[x], w[y], w[z])) ++bad;
+                }
+            }
+        }
+        printf("split total=%ld bad=%ld\n", total, bad);
         return bad == 0 ? 0 : 1;
     }
     if (std::string(mode) == "triples") {

@@ -35,6 +35,11 @@ def test_triple_list_and_decoder(math_check):
     assert out.returncode == 0, out.stdout + out.stderr
 
 
+def test_split_cycle_fields_match_recount(math_check):
+    out = subprocess.run([math_check, "split"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+
+
 def test_tight_bound_is_sound(math_check):
     out = subprocess.run([math_check, "tight"], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
