@@ -36,7 +36,7 @@ HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes (read + write) per expanded node of the search kernel, from an ncu capture of a
 # config-1 batch of 64 instances (1.18 GB for 1.86 M nodes); the bench scales it by the nodes
 # of its own launches, since its workload is too large to capture under ncu.
-NCU_DRAM_BYTES_PER_NODE = 634.0
+NCU_DRAM_BYTES_PER_NODE = 1440.0  # one config-2 m=8 case, profiles/search_engine_config2_single_m8.md
 
 
 def parse_args():
@@ -314,8 +314,9 @@ def run_ours(args):
                      "frac": round(achieved / peak, 6),
                      "traffic": round(NCU_DRAM_BYTES_PER_NODE * nodes / launches, 1) if launches else None,
                      "note": f"algorithmic table/task/instance bytes over kernel time; peak {peak_kind}; traffic = "
-                             "DRAM bytes per launch scaled from an ncu capture by expanded nodes; the kernel is "
-                             "issue/latency bound (ncu issue-active 13.6%, DRAM throughput 0.15%)"},
+                             "DRAM bytes per launch scaled from an ncu capture (1.44 kB per expanded node) by the "
+                             "launch's nodes; the kernel is bound by table-probe latency and warp count (ncu: "
+                             "issue-active 29%, DRAM throughput 3.5%, long-scoreboard and fence stalls on top)"},
         "e2e": {"value": round(cases / wall, 3) if wall > 0 else None, "unit": "cases/s",
                 "h2d_bytes_per_step": args.batch * 144, "d2h_bytes_per_step": args.batch * 96},
         "clocks": clocks.summary(),
