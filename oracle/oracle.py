@@ -43,6 +43,12 @@ def lib() -> ctypes.CDLL:
         L.oracle_pi_filter.argtypes = [_u8p, ctypes.c_int, _u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _u8p,
                                        ctypes.c_int64]
         L.oracle_pi_filter_keep.argtypes = [_u8p, ctypes.c_int, _u8p, ctypes.c_int, _u8p, ctypes.c_int, ctypes.c_int]
+        _f32p = ctypes.POINTER(ctypes.c_float)
+        L.oracle_signature.argtypes = [_u8p, ctypes.c_int, _f32p]
+        L.oracle_equivalent_signatures.argtypes = [_u8p, ctypes.c_int, _f32p]
+        L.oracle_signature_hash.argtypes = [_f32p, ctypes.c_int]
+        L.oracle_signature_hash.restype = ctypes.c_int32
+        L.oracle_canonical.argtypes = [_u8p, ctypes.c_int, _f32p, _i32p, _i32p]
         _lib = L
     return _lib
 
@@ -116,3 +122,44 @@ def pi_filter(cycle, triple, n, skip_2move, max_out=1 << 20):
 def pi_filter_keep(pi, cycle, triple, skip_2move) -> bool:
     return bool(lib().oracle_pi_filter_keep(_u8(pi), len(pi), _u8(cycle), len(cycle), _u8(triple), len(triple),
                                             1 if skip_2move else 0))
+
+
+def parse_cycles(text: str):
+    """Successor array of a permutation written in cycle notation, e.g. "(0 9 7)(1 5 2 6 3)";
+    n is the largest symbol + 1 (the reference's configurations cover every symbol)."""
+    import re
+    cycles = [[int(t) for t in grp.replace(",", " ").split()] for grp in re.findall(r"\(([^()]*)\)", text)]
+    n = max(max(c) for c in cycles) + 1
+    succ = list(range(n))
+    for c in cycles:
+        for i, x in enumerate(c):
+            succ[x] = c[(i + 1) % len(c)]
+    return succ
+
+
+def signature(spi):
+    n = len(spi)
+    out = (ctypes.c_float * n)()
+    assert lib().oracle_signature(_u8(spi), n, out) == 0
+    return list(out)
+
+
+def equivalent_signatures(spi):
+    n = len(spi)
+    out = (ctypes.c_float * (2 * n * n))()
+    assert lib().oracle_equivalent_signatures(_u8(spi), n, out) == 0
+    return [list(out[v * n:(v + 1) * n]) for v in range(2 * n)]
+
+
+def signature_hash(sig) -> int:
+    arr = (ctypes.c_float * len(sig))(*sig)
+    return int(lib().oracle_signature_hash(arr, len(sig)))
+
+
+def canonical(spi):
+    """(canonical signature, hash code, variant index) of Configuration.getCanonical."""
+    n = len(spi)
+    out = (ctypes.c_float * n)()
+    h, v = ctypes.c_int32(), ctypes.c_int32()
+    assert lib().oracle_canonical(_u8(spi), n, out, ctypes.byref(h), ctypes.byref(v)) == 0
+    return list(out), h.value, v.value

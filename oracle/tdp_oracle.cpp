@@ -572,3 +572,153 @@ extern "C" int64_t oracle_extension_filter(const uint8_t *spi, const uint8_t *pi
         }
     return hits;
 }
+
+// ---- configuration signatures and canonical form: Configuration.java -----------------
+//
+// A configuration is spi over symbols 0..n-1 (every symbol in a cycle of length >= 2, as
+// the reference requires: Configuration.signature dereferences each symbol's cycle) with pi
+// the n-cycle (0 1 ... n-1) (CANONICAL_PI, CommonOperations.java:26-33).  spi is given as
+// its successor array: spi[x] is the symbol after x in x's cycle.
+
+namespace {
+
+// Configuration.signature (Configuration.java:56-104) for spi (successor array) and the pi
+// cycle written as the array pic[0..n-1].  Labels number the cycles by first appearance
+// along pi; a cycle is oriented when its symbols are not in cyclic order in pi^-1
+// (CommonOperations.java:167-182 on the reversed pi); an oriented cycle's symbols are
+// numbered 1.. along the cycle from the one at the smallest pi position; the value is
+// label + index / 100 in float arithmetic.
+void signature_of(const int *spi, const int *pic, int n, float *out) {
+    int pos[kMaxN + 2], label[kMaxN + 2], orient[kMaxN + 2], cyc[kMaxN + 2];
+    for (int i = 0; i < n; ++i) pos[pic[i]] = i;
+    // cycle id = smallest symbol of the cycle
+    for (int x = 0; x < n; ++x) {
+        int m = x;
+        for (int y = spi[x]; y != x; y = spi[y]) m = std::min(m, y);
+        cyc[x] = m;
+    }
+    for (int x = 0; x < n; ++x) label[x] = 0, orient[x] = -1;
+    int next = 1;
+    for (int i = 0; i < n; ++i) {
+        const int s = pic[i], c = cyc[s];
+        if (orient[c] < 0) {
+            // cyclic order in pi^-1: index in the reversed pi array is n-1-pos
+            int leaps = 0;
+            int y = c;
+            do {
+                const int z = spi[y];
+                if ((n - 1 - pos[y]) > (n - 1 - pos[z])) ++leaps;
+                y = z;
+            } while (y != c);
+            orient[c] = leaps > 1 ? 1 : 0;
+        }
+        if (label[c] == 0) label[c] = next++;
+        float v = (float)label[c];
+        if (orient[c]) {
+            // anchor: the cycle's symbol with the smallest pi position
+            int anchor = c;
+            int y = c;
+            do {
+                if (pos[y] < pos[anchor]) anchor = y;
+                y = spi[y];
+            } while (y != c);
+            int idx = 1;
+            for (int z = anchor; z != s; z = spi[z]) ++idx;
+            v = (float)label[c] + (float)idx / 100.0f;
+        }
+        out[i] = v;
+    }
+}
+
+// java.util.zip.CRC32 over the big-endian bytes of each float (Signature.hashCode,
+// Configuration.java:290-303), as a signed int.
+int32_t signature_hash(const float *sig, int n) {
+    uint32_t crc = 0xFFFFFFFFu;
+    for (int i = 0; i < n; ++i) {
+        uint32_t bits;
+        std::memcpy(&bits, &sig[i], 4);
+        for (int b = 3; b >= 0; --b) {
+            crc ^= (bits >> (8 * b)) & 0xFFu;
+            for (int k = 0; k < 8; ++k) crc = (crc >> 1) ^ (0xEDB88320u & (0u - (crc & 1u)));
+        }
+    }
+    return (int32_t)(crc ^ 0xFFFFFFFFu);
+}
+
+// Arrays.compare on float[] (Float.compare per element; equal lengths here).
+int compare_signatures(const float *a, const float *b, int n) {
+    for (int i = 0; i < n; ++i) {
+        if (a[i] < b[i]) return -1;
+        if (a[i] > b[i]) return 1;
+    }
+    return 0;
+}
+
+// Variant v of getEquivalentSignatures (Configuration.java:180-186): v = 2r is pi started
+// at symbol r, v = 2r+1 its mirror (Configuration.java:188-195): spi conjugated by the
+// involution swapping the symbols at pi positions i and n-1-i, then inverted.
+void equivalent_signature(const int *spi, int n, int v, float *out) {
+    const int r = v >> 1;
+    int pic[kMaxN + 2];
+    for (int i = 0; i < n; ++i) pic[i] = (r + i) % n;
+    if ((v & 1) == 0) {
+        signature_of(spi, pic, n, out);
+        return;
+    }
+    int pos[kMaxN + 2], conj[kMaxN + 2], inv[kMaxN + 2], m[kMaxN + 2];
+    for (int i = 0; i < n; ++i) pos[pic[i]] = i;
+    for (int x = 0; x < n; ++x) conj[x] = pic[n - 1 - pos[x]];
+    for (int x = 0; x < n; ++x) inv[spi[x]] = x;
+    for (int x = 0; x < n; ++x) m[x] = conj[inv[conj[x]]];  // (c spi c)^-1
+    signature_of(m, pic, n, out);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Signature of spi (successor array) under CANONICAL_PI.  Returns 0, or -1 on bad input.
+int oracle_signature(const uint8_t *spi, int n, float *out) {
+    if (n < 2 || n > kMaxN) return -1;
+    int s[kMaxN + 2], pic[kMaxN + 2];
+    for (int i = 0; i < n; ++i) s[i] = spi[i], pic[i] = i;
+    signature_of(s, pic, n, out);
+    return 0;
+}
+
+// All 2n equivalent signatures, variant v at out + v*n.
+int oracle_equivalent_signatures(const uint8_t *spi, int n, float *out) {
+    if (n < 2 || n > kMaxN) return -1;
+    int s[kMaxN + 2];
+    for (int i = 0; i < n; ++i) s[i] = spi[i];
+    for (int v = 0; v < 2 * n; ++v) equivalent_signature(s, n, v, out + (size_t)v * n);
+    return 0;
+}
+
+int32_t oracle_signature_hash(const float *sig, int n) { return signature_hash(sig, n); }
+
+// Configuration.getCanonical / hashCode (Configuration.java:147-174, 241-245): the
+// equivalent signature with the least hash (signed), ties broken by Arrays.compare.
+// Writes it to outSig, its hash to *outHash and its variant index to *outVariant.
+int oracle_canonical(const uint8_t *spi, int n, float *outSig, int32_t *outHash, int32_t *outVariant) {
+    if (n < 2 || n > kMaxN) return -1;
+    int s[kMaxN + 2];
+    for (int i = 0; i < n; ++i) s[i] = spi[i];
+    float cur[kMaxN + 2];
+    int32_t best = INT32_MAX;
+    int bestV = -1;
+    for (int v = 0; v < 2 * n; ++v) {
+        equivalent_signature(s, n, v, cur);
+        const int32_t h = signature_hash(cur, n);
+        if (bestV < 0 || h < best || (h == best && compare_signatures(cur, outSig, n) < 0)) {
+            best = h;
+            bestV = v;
+            std::memcpy(outSig, cur, sizeof(float) * (size_t)n);
+        }
+    }
+    *outHash = best;
+    *outVariant = bestV;
+    return 0;
+}
+
+}  // extern "C"
