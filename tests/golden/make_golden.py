@@ -8,7 +8,7 @@ Outputs (small JSON files, committed):
   cases_3_2.json       src/main/resources/cases/cases-3,2.txt        (ratio 1.5)
   cases_7cycle.json    src/main/resources/cases/cases-oriented-7cycle.txt
 Each record: {"spi": one-line spi (n bytes), "pi": pi array, "moves": [[a,b,c], ...] symbol
-3-cycles}.  pi is the identity array except for the oriented 7-cycle file, whose left side is
+3-cycles, "line": the case line as written in the file}.  pi is the identity array except for the oriented 7-cycle file, whose left side is
 pi itself with spi = (0 3 4 1 5 2 6) (Silvaetal.java:151-165).
 The text format is the one parsed by AbstractSbtAlgorithm.java:166-179: "cycles->[moves]".
 """
@@ -58,7 +58,7 @@ def main(ref: str) -> None:
                 else:
                     spi = one_line(parse_cycles(left))
                     pi = list(range(len(spi)))
-                records.append({"spi": spi, "pi": pi, "moves": parse_cycles(right)})
+                records.append({"spi": spi, "pi": pi, "moves": parse_cycles(right), "line": line})
         with open(os.path.join(here, out), "w") as fh:
             json.dump({"source": rel, "records": records}, fh, separators=(",", ":"))
         print(out, len(records))
