@@ -137,6 +137,21 @@ int tdp_set_engine_config(int slot, const tdp_engine_config *cfg);
 
 int tdp_device_count(void);
 
+/* ---- batched canonical form (replaces Configuration.getCanonical / hashCode,
+ * Configuration.java:147-195, 241-245, 290-303, for many configurations at once) --------
+ * Row r is spi over n[r] symbols (2 <= n[r] <= 63) as a 64-byte successor array
+ * (spi[x] = the symbol after x in its cycle; every symbol in a cycle of length >= 2), with
+ * pi = (0 1 ... n-1).  For each row: the canonical signature (64 floats, the first n[r]
+ * used: cycle label, plus index/100 on oriented cycles), its hash code (CRC32 of the
+ * big-endian float bytes as a signed int, equal to Configuration.hashCode) and the variant
+ * that produced it (2r: pi started at symbol r; 2r+1: its mirror).  tdp_canonical takes
+ * host buffers and validates the rows (TDP_ERR_ARGUMENT on a bad row); the _device form
+ * takes device buffers on `stream` and does not validate. */
+int tdp_canonical(const uint8_t *spi, const uint8_t *n, int count, float *signature, int32_t *hash_code,
+                  int32_t *variant);
+int tdp_canonical_device(const uint8_t *spi, const uint8_t *n, int count, float *signature, int32_t *hash_code,
+                         int32_t *variant, void *stream);
+
 /* ---- batched extension filter (no counterpart in the reference) -----------------------
  * Applies the permutation-filter predicates of tdp_pi_filter to every extension of `count`
  * base configurations (spi/pi rows of 64 bytes, n symbols each, 3 <= n <= 60) that adds one

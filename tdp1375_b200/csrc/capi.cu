@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/tdp1375.h"
+#include "canonical.h"
 #include "extension_filter.h"
 #include "pi_filter.h"
 #include "search_engine.h"
@@ -401,4 +402,53 @@ extern "C" int64_t tdp_extension_filter(const uint8_t *spi, const uint8_t *pi, i
     int64_t hits = 0;
     for (size_t i = 0; i < total; ++i) hits += keep[i];
     return hits;
+}
+
+extern "C" int tdp_canonical_device(const uint8_t *spi, const uint8_t *n, int count, float *signature,
+                                    int32_t *hash_code, int32_t *variant, void *stream) {
+    std::string err;
+    const int rc = tdp::canonical_device(spi, n, count, signature, hash_code, variant,
+                                         static_cast<cudaStream_t>(stream), err);
+    if (rc != 0) return fail(rc == -1 ? TDP_ERR_ARGUMENT : TDP_ERR_CUDA, err);
+    return 0;
+}
+
+extern "C" int tdp_canonical(const uint8_t *spi, const uint8_t *n, int count, float *signature, int32_t *hash_code,
+                             int32_t *variant) {
+    if (count < 0 || (count > 0 && (!spi || !n || !signature || !hash_code || !variant)))
+        return fail(TDP_ERR_ARGUMENT, "tdp_canonical: bad buffers");
+    if (count == 0) return 0;
+    std::string err;
+    if (tdp::canonical_validate(spi, n, count, err) != 0) return fail(TDP_ERR_ARGUMENT, err);
+    const size_t rows = (size_t)count * 64;
+    uint8_t *dSpi = nullptr, *dN = nullptr;
+    float *dSig = nullptr;
+    int32_t *dHash = nullptr, *dVar = nullptr;
+    auto release = [&] {
+        cudaFree(dSpi);
+        cudaFree(dN);
+        cudaFree(dSig);
+        cudaFree(dHash);
+        cudaFree(dVar);
+    };
+    if (cudaMalloc(&dSpi, rows) != cudaSuccess || cudaMalloc(&dN, (size_t)count) != cudaSuccess ||
+        cudaMalloc(&dSig, rows * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&dHash, (size_t)count * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&dVar, (size_t)count * sizeof(int32_t)) != cudaSuccess) {
+        release();
+        return fail(TDP_ERR_OUT_OF_MEMORY, "tdp_canonical: device allocation failed");
+    }
+    int rc = 0;
+    if (cudaMemcpy(dSpi, spi, rows, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dN, n, (size_t)count, cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = -3, err = "tdp_canonical: upload failed";
+    if (rc == 0) rc = tdp::canonical_device(dSpi, dN, count, dSig, dHash, dVar, nullptr, err);
+    if (rc == 0 && (cudaMemcpy(signature, dSig, rows * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess ||
+                    cudaMemcpy(hash_code, dHash, (size_t)count * sizeof(int32_t), cudaMemcpyDeviceToHost) !=
+                        cudaSuccess ||
+                    cudaMemcpy(variant, dVar, (size_t)count * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess))
+        rc = -3, err = "tdp_canonical: download failed";
+    release();
+    if (rc != 0) return fail(rc == -1 ? TDP_ERR_ARGUMENT : TDP_ERR_CUDA, err);
+    return 0;
 }

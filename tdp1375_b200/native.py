@@ -80,6 +80,8 @@ SIGNATURES = {
     "tdp_mlp_error": (ctypes.c_int, []),
     "tdp_set_order_model": (ctypes.c_int, [ctypes.c_int] + [vp] * 8),
     "tdp_enable_order_model": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "tdp_canonical": (ctypes.c_int, [vp, vp, ctypes.c_int, vp, vp, vp]),
+    "tdp_canonical_device": (ctypes.c_int, [vp, vp, ctypes.c_int, vp, vp, vp, vp]),
     "tdp_extension_count": (ctypes.c_int, [ctypes.c_int]),
     "tdp_extension_filter": (ctypes.c_int64, [vp, vp, ctypes.c_int, ctypes.c_int, vp]),
     "tdp_extension_filter_device": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]),

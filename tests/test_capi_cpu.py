@@ -54,3 +54,23 @@ def test_pi_filter_argument_errors(native_lib):
     assert native_lib.tdp_pi_filter(cyc, 3, tri, 3, 64, 0, out, 1) == native.ERR_ARGUMENT
     assert native_lib.tdp_pi_filter(cyc, 3, tri, 3, 5, 0, out, 1) == native.ERR_ARGUMENT
     assert "out of range" in native.last_error()
+
+
+def test_canonical_rejects_bad_rows(native_lib):
+    """Rows are validated on the host before any device work."""
+    import numpy as np
+    from tdp1375_b200 import native
+    vp = ctypes.c_void_p
+    spi = np.zeros((1, 64), np.uint8)
+    spi[0, :4] = [1, 0, 2, 3]  # fixed points 2 and 3
+    ns = np.array([4], np.uint8)
+    sig = np.zeros((1, 64), np.float32)
+    h = np.zeros(1, np.int32)
+    v = np.zeros(1, np.int32)
+    rc = native_lib.tdp_canonical(spi.ctypes.data_as(vp), ns.ctypes.data_as(vp), 1, sig.ctypes.data_as(vp),
+                                  h.ctypes.data_as(vp), v.ctypes.data_as(vp))
+    assert rc == native.ERR_ARGUMENT and "fixed points" in native.last_error()
+    ns[0] = 64
+    rc = native_lib.tdp_canonical(spi.ctypes.data_as(vp), ns.ctypes.data_as(vp), 1, sig.ctypes.data_as(vp),
+                                  h.ctypes.data_as(vp), v.ctypes.data_as(vp))
+    assert rc == native.ERR_ARGUMENT and "2..63" in native.last_error()
