@@ -1,6 +1,6 @@
 """Batched uneven search: one persistent, graph-captured launch over many instances.
 
-    python -m tdp1375_b200.batched_eval [--count 1000000] [--sample 20000] [--out result.json]
+    python -m tdp1375_b200.batched_eval [--count 1000000] [--sample 100000] [--out result.json]
 
 Instances come from the seeded uneven generator: 3-permutations with m truncated-geometric
 on 3..10 (p = 0.35) mixed with 10% random permutations of n' = 20..30 (pi = 0 followed by a
@@ -41,7 +41,7 @@ def instances(count: int):
 def main(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--count", type=int, default=1_000_000)
-    p.add_argument("--sample", type=int, default=20_000)
+    p.add_argument("--sample", type=int, default=100_000)
     p.add_argument("--table-entries", type=int, default=1 << 30)
     p.add_argument("--depth", type=int, default=11)
     p.add_argument("--tune-cache", default="")
@@ -66,7 +66,7 @@ def main(argv=None):
         choice = None  # cached before this tunable existed
     if choice is None:
         sample = api.make_instances(cases[: args.sample], args.depth, False)
-        space = {"poll_interval": [16, 32, 64], "sparse_enumeration": [2], "warps_per_instance": [0, 2, 8]}
+        space = {"poll_interval": [16, 32, 64], "sparse_enumeration": [2], "warps_per_instance": [0, 4, 8]}
         choice = autotune.tune(WORKLOAD, sample, min(args.sample, len(cases)), rate,
                                table_sizes=(1 << 28, args.table_entries), space=space, cache_path=cache_path)
 
