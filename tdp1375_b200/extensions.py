@@ -15,6 +15,9 @@ the reference has them).
   a <= b; kept when it stays unoriented with at most two open gates, or, for a 3-cycle that
   turns into an oriented 5-cycle, when that 5-cycle admits no 2-move (Extensions.java:143-196).
 
+* ``combination_extensions``: a bad small component (oriented 5-cycle, interleaving pair,
+  necklaces) inserted at every position (Combinations.java:31-46, 182-199).
+
 Each extension is returned as (description, spi) with spi = Configuration.ofSignature of
 the extended signature.
 """
@@ -244,4 +247,40 @@ def type3_extensions(spi: Sequence[int]) -> List[Tuple[str, List[int]]]:
                     fractions = [F(F(x) + F(label)) for x in (0.01, 0.03, 0.05, 0.02, 0.04)]
                     if _float_cyclic(prime, fractions):  # otherwise it admits a 2-move
                         out.append((f"a={a} b={b}, extended cycle: {cycle_text}, turn oriented", of_signature(prime)))
+    return out
+
+
+# Combinations.java:31-46: the bad small components, in the reference's order.
+BAD_SMALL_COMPONENTS = [
+    "(0,3,1,4,2)",                                   # oriented 5-cycle
+    "(0,4,2)(1,5,3)",                                # interleaving pair
+    "(0,10,2)(1,5,3)(4,8,6)(7,11,9)",                # necklace of size 4
+    "(0,7,5)(1,11,9)(2,6,4)(3,10,8)",                # twisted necklace of size 4
+    "(0,4,2)(1,14,12)(3,7,5)(6,10,8)(9,13,11)",      # necklace of size 5
+    "(0,16,2)(1,5,3)(4,8,6)(7,11,9)(10,14,12)(13,17,15)",  # necklace of size 6
+]
+
+
+def _successor_of(text: str) -> List[int]:
+    import re
+    cycles = [[int(t) for t in g.replace(",", " ").split()] for g in re.findall(r"\(([^()]*)\)", text)]
+    n = max(max(c) for c in cycles) + 1
+    succ = list(range(n))
+    for c in cycles:
+        for i, x in enumerate(c):
+            succ[x] = c[(i + 1) % len(c)]
+    return succ
+
+
+def combination_extensions(spi: Sequence[int]) -> List[Tuple[str, List[int]]]:
+    """SortOrExtendCombinations.extendCombinations (Combinations.java:182-199): for every bad
+    small component and every position i < n, the component's signature with the
+    configuration's cycle count added to each value (float) inserted at i."""
+    sig = signature(spi)
+    cycles = len(cycles_in_order(spi))
+    out = []
+    for b, text in enumerate(BAD_SMALL_COMPONENTS):
+        comp = [F(v + F(cycles)) for v in signature(_successor_of(text))]
+        for i in range(len(sig)):
+            out.append((f"component={b} i={i}", of_signature(list(sig[:i]) + comp + list(sig[i:]))))
     return out

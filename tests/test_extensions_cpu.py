@@ -71,3 +71,16 @@ def test_extension_structure(oracle, rec):
         assert len(grown) == len(lengths) and sum(grown) == n + 2
         if "turn oriented" in desc:
             assert 5 in grown and 3 in lengths
+
+
+@pytest.mark.parametrize("rec", GOLDEN, ids=[r["spi"] for r in GOLDEN])
+def test_combination_extensions_structure(oracle, rec):
+    spi = oracle.parse_cycles(rec["spi"])
+    n, lengths = len(spi), cycle_lengths(spi)
+    out = X.combination_extensions(spi)
+    assert len(out) == len(X.BAD_SMALL_COMPONENTS) * n
+    for desc, ext in out:
+        b = int(desc.split()[0].split("=")[1])
+        comp = X._successor_of(X.BAD_SMALL_COMPONENTS[b])
+        assert sorted(ext) == list(range(n + len(comp)))
+        assert cycle_lengths(ext) == sorted(lengths + cycle_lengths(comp))
