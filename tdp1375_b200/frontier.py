@@ -72,7 +72,6 @@ class Resolution:
     found: bool
     moves: List[Tuple[int, int, int]] = field(default_factory=list)  # symbol 3-cycles on spi
     depth_limit: int = 0            # max depth of the stage that decided it
-    searched: bool = False          # searched by this call (not a duplicate or earlier result)
 
 
 class Frontier:
@@ -81,7 +80,8 @@ class Frontier:
         self.min_rate = np.float32(2) / np.float32(max_ratio)
         self.max_depth = max_depth
         self.decided: Dict[bytes, Resolution] = {}
-        self.stage_counts: List[Tuple[int, int, int]] = []  # (depth limit, searched, found) per stage
+        self.stage_counts: List[Tuple[int, int, int]] = []  # (stage, searched, found) per stage
+        self.last_new: List[Resolution] = []  # configurations first decided by the last call
 
     def _stages(self, ub: int) -> List[int]:
         out = [4]
@@ -99,7 +99,7 @@ class Frontier:
             k = keys[r]
             if k in self.decided or k in todo:
                 continue
-            todo[k] = Resolution(k, int(hashes[r]), canonical_spi(s, int(variants[r])), False, searched=True)
+            todo[k] = Resolution(k, int(hashes[r]), canonical_spi(s, int(variants[r])), False)
         pending = list(todo.values())
         stage = 0
         while pending:
@@ -131,6 +131,7 @@ class Frontier:
             pending = [res for res in batch if not res.found]
             stage += 1
         self.decided.update(todo)
+        self.last_new = list(todo.values())
         return [self.decided[k] for k in keys]
 
 
