@@ -196,17 +196,16 @@ __device__ __forceinline__ uint64_t key_hash(const uint64_t (&k)[KW], uint32_t t
     return h;
 }
 
-struct LaneStats {
-    unsigned probes = 0, pruned = 0, inserts = 0, full = 0;
-};
+// Outcome bits of dedup_admit: admitted, inserted into an empty or reclaimed entry, or
+// admitted without an entry because the window was full.
+constexpr uint32_t kAdmitted = 1u, kInserted = 2u, kWindowFull = 4u;
 
 // Transposition-table admission (sorting_search.cu:261-298 semantics, per instance).
 template <int KW>
-__device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t generation, uint32_t tag,
-                                            const uint64_t (&key)[KW], uint64_t h, uint32_t depth, LaneStats &ls) {
+__device__ __forceinline__ uint32_t dedup_admit(const EngineParams &P, uint32_t generation, uint32_t tag,
+                                            const uint64_t (&key)[KW], uint64_t h, uint32_t depth) {
     auto *table = reinterpret_cast<DedupEntry<KW> *>(P.table);
     const uint32_t base = (uint32_t)(h >> 24) & P.tableMask & ~7u;
-    ++ls.probes;
     // Eight independent relaxed tag loads (one round trip); only when a tag matches does the
     // lane pay an acquire fence before reading keys, which pairs with the release store that
     // published the entry.  (Eight acquire loads would serialise into eight round trips.)
@@ -229,17 +228,10 @@ __device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t gene
             // Best depths only decrease, so a value read after the fence that is already
             // <= depth decides the prune without an atomic.
             const uint32_t seen = ld_relaxed_u32(&e->depth);
-            if (eq && seen <= depth) {
-                ++ls.pruned;
-                return false;
-            }
+            if (eq && seen <= depth) return 0u;
             if (eq) {
                 const uint32_t prev = atomicMin(&e->depth, depth);
-                if (prev <= depth) {
-                    ++ls.pruned;
-                    return false;
-                }
-                return true;
+                return prev <= depth ? 0u : kAdmitted;
             }
         } else if (t == 0u || (t != kTagWriting && (t >> kInstanceBits) != generation)) {
             freeMask |= 1u << q;
@@ -269,12 +261,11 @@ __device__ __forceinline__ bool dedup_admit(const EngineParams &P, uint32_t gene
 #pragma unroll
             for (int kq = 0; kq < KW; ++kq) __stcg(&e->key[kq], key[kq]);
             st_release_u32(&e->tag, tag);  // the release orders the depth and key stores before it
-            ++ls.inserts;
+            return kAdmitted | kInserted;
         }
-    } else {
-        ++ls.full;
+        return kAdmitted;
     }
-    return true;
+    return kAdmitted | kWindowFull;
 }
 
 // Idle-warp ring: a bounded lock-free multi-producer/multi-consumer queue of warp ids.  Slot
@@ -481,16 +472,29 @@ __device__ __forceinline__ uint32_t triple_at(const SparseFrame &sf, int u) {
     return pack_triple((uint32_t)p, q, r);
 }
 
+// Saved state of a DFS frame, written when the warp descends from it (one writer lane).
+template <int KW>
+struct FrameRec {
+    int cursor, end, chunk, even, step;  // next chunk, range end, chunk of `pending`, odd-cycle count, chunk step
+    uint32_t pending;                    // admitted children of chunk `chunk` not yet descended into
+    uint32_t move;                       // move that left this frame (the path)
+    uint32_t pad;
+    uint64_t key[KW];                    // transposition-table key of the frame's node
+};
+
 template <int NW>
 struct WarpShared {
     uint32_t words[kMaxDepth + 1][NW * 32];
+    FrameRec<KeyTraits<NW>::KW> frames[kMaxDepth + 1];
     uint32_t tri[NW == 1 ? kMaxTriples : 1];  // triple list of the frame being enumerated
+    uint64_t rules[32];                       // success (0..15) and expansion (16..31) tables of the instance
+    unsigned long long taskNodes, taskChildren;  // counters of the task in hand
     uint32_t staging[52];
     unsigned long long stats[kStatCount];  // per-warp counters, flushed once at exit
 };
 
 template <int NW>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_engine_kernel(const EngineParams P) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_engine_kernel(const EngineParams P) {
     using K = KeyTraits<NW>;
     constexpr int KW = K::KW;
     __shared__ WarpShared<NW> smem[kWarpsPerBlock];
@@ -502,7 +506,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
 
     if (lane < kStatCount) S.stats[lane] = 0ull;
     __syncwarp();
-    LaneStats ls;
     const uint32_t gw = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     bool registered = false;
     int backoff = 64;
@@ -574,8 +577,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         uint32_t inst;
         int baseDepth, even, lo, hi;
         uint32_t w[NW];
-        uint32_t fMove = 0;
-        unsigned long long tNodes = 0, tChildren = 0;
         if (kind == 1) {
             __threadfence();  // every lane reads the task only after lane 0 observed the flag
             const uint32_t *src = reinterpret_cast<const uint32_t *>(&P.mail[gw].task);
@@ -593,8 +594,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
             even = (int)((S.staging[1] >> 8) & 0xFFu);
             lo = (int)(S.staging[2] & 0xFFFFu);
             hi = (int)(S.staging[2] >> 16);
-            if (S.staging[3] & 1u) tNodes = 1;
-            if (lane < baseDepth) fMove = S.staging[4 + lane];
+            if (lane == 0) S.taskNodes = S.staging[3] & 1u;
+            if (lane < baseDepth) S.frames[lane].move = S.staging[4 + lane];
             const uint8_t *bytes = reinterpret_cast<const uint8_t *>(S.staging);
             const int n = P.in[inst].n;
 #pragma unroll
@@ -620,14 +621,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                 const int x = lane + 32 * h;
                 w[h] = (x < n) ? ((uint32_t)I->spi[x] | ((uint32_t)I->pi[x] << 6)) : 0u;
             }
-            tNodes = 1;
+            if (lane == 0) S.taskNodes = 1;
         }
+        if (lane == 0) S.taskChildren = 0;
         const int n = P.in[inst].n;
         const int T = combinations3(n);
         const uint32_t *trip = P.triples + combinations4(n);
         const uint32_t tag = (generation << kInstanceBits) | inst;
         const RuleTable *rt = P.rules + P.in[inst].rule;
-        const uint64_t ruleReg = (lane < 16) ? rt->sat[lane] : rt->expand[lane - 16];
+        S.rules[lane] = (lane < 16) ? rt->sat[lane] : rt->expand[lane - 16];
+        __syncwarp();
 
         build_tables<NW>(w, n, lane);
         uint64_t key[KW];
@@ -636,15 +639,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         int f = baseDepth;
         int cursor = lo, end = hi, chunk = 0;
         uint32_t pending = 0;
-        int fCursor = 0, fEnd = 0, fChunk = 0, fEven = 0, fStep = 32;
-        uint32_t fPending = 0;
-        uint64_t fKey[KW];
-#pragma unroll
-        for (int q = 0; q < KW; ++q) fKey[q] = 0;
 #pragma unroll
         for (int h = 0; h < NW; ++h) S.words[f][h * 32 + lane] = w[h];
-        uint64_t satMask = shfl64(ruleReg, f + 1);
-        uint64_t expMask = shfl64(ruleReg, 16 + f + 1);
+        uint64_t satMask = S.rules[f + 1];
+        uint64_t expMask = S.rules[16 + f + 1];
         // The root of an instance with a learned order enumerates its children in that order
         // (dense mode, index space = positions in the order).
         const uint16_t *rootOrder = (P.order && NW == 1) ? P.order + (size_t)inst * (size_t)P.orderStride : nullptr;
@@ -666,20 +664,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                 if (cursor >= end) {
                     if (f == baseDepth) break;
                     --f;
-                    cursor = __shfl_sync(kFull, fCursor, f);
-                    end = __shfl_sync(kFull, fEnd, f);
-                    pending = __shfl_sync(kFull, fPending, f);
+                    const FrameRec<KW> &fr = S.frames[f];
+                    cursor = fr.cursor;
+                    end = fr.end;
+                    pending = fr.pending;
                     // An exhausted parent is left at once: its words, key and enumeration
                     // state are not needed.
                     if (pending == 0u && cursor >= end) continue;
-                    chunk = __shfl_sync(kFull, fChunk, f);
-                    even = __shfl_sync(kFull, fEven, f);
+                    chunk = fr.chunk;
+                    even = fr.even;
 #pragma unroll
-                    for (int q = 0; q < KW; ++q) key[q] = shfl64(fKey[q], f);
+                    for (int q = 0; q < KW; ++q) key[q] = fr.key[q];
 #pragma unroll
                     for (int h = 0; h < NW; ++h) w[h] = S.words[f][h * 32 + lane];
-                    satMask = shfl64(ruleReg, f + 1);
-                    expMask = shfl64(ruleReg, 16 + f + 1);
+                    satMask = S.rules[f + 1];
+                    expMask = S.rules[16 + f + 1];
                     sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, (rootOrder && f == 0) ? 0 : P.sparse,
                                           S.tri);
                     continue;
@@ -721,8 +720,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                         int remChunks = 0;
                         uint32_t pend = 0u;
                         if (lane >= baseDepth && lane < f) {
-                            remChunks = (fEnd - fCursor + fStep - 1) / fStep;
-                            pend = fPending;
+                            const FrameRec<KW> &fr = S.frames[lane];
+                            remChunks = (fr.end - fr.cursor + fr.step - 1) / fr.step;
+                            pend = fr.pending;
                         }
                         if (lane == f) {
                             remChunks = (end - cursor + step - 1) / step;
@@ -750,17 +750,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                         target = __shfl_sync(kFull, target, 0);
                         if (target >= 0) {
                             Task *tk = &P.mail[target].task;
-                            const int gEven = __shfl_sync(kFull, (lane == f) ? even : fEven, g);
+                            const int gEven = (g == f) ? even : S.frames[g].even;
                             uint32_t hdr1, hdr2, hdr3;
                             if (mode == 2) {
-                                const int gChunk = __shfl_sync(kFull, (lane == f) ? chunk : fChunk, g);
+                                const int gChunk = (g == f) ? chunk : S.frames[g].chunk;
                                 const uint32_t gPend = __shfl_sync(kFull, pend, g);
                                 const int l = __ffs(gPend) - 1;
                                 uint32_t wg[NW];
 #pragma unroll
                                 for (int h = 0; h < NW; ++h) wg[h] = S.words[g][h * 32 + lane];
-                                const uint64_t gSat = shfl64(ruleReg, g + 1);
-                                const uint64_t gExp = shfl64(ruleReg, 16 + g + 1);
+                                const uint64_t gSat = S.rules[g + 1];
+                                const uint64_t gExp = S.rules[16 + g + 1];
                                 const SparseFrame gsf =
                                     sparse_setup<NW>(wg, n, lane, gEven, gSat, gExp, (rootOrder && g == 0) ? 0 : P.sparse,
                                                      nullptr);
@@ -794,7 +794,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                                         tk->pi[x] = (uint8_t)w_pi(cw[h]);
                                     }
                                 }
-                                if (lane < g) tk->path[lane] = fMove;
+                                if (lane < g) tk->path[lane] = S.frames[lane].move;
                                 if (lane == g) tk->path[g] = ctr;
                                 hdr1 = (uint32_t)(g + 1) | ((uint32_t)cEven << 8);
                                 hdr2 = 0xFFFFu << 16;
@@ -802,13 +802,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                                 const uint32_t bit = 1u << l;
                                 if (g == f) {
                                     pending &= ~bit;
-                                } else if (lane == g) {
-                                    fPending &= ~bit;
+                                } else if (lane == 0) {
+                                    S.frames[g].pending &= ~bit;
                                 }
                             } else {
-                                const int gc = __shfl_sync(kFull, (lane == f) ? cursor : fCursor, g);
-                                const int ge = __shfl_sync(kFull, (lane == f) ? end : fEnd, g);
-                                const int gStep = __shfl_sync(kFull, (lane == f) ? step : fStep, g);
+                                const int gc = (g == f) ? cursor : S.frames[g].cursor;
+                                const int ge = (g == f) ? end : S.frames[g].end;
+                                const int gStep = (g == f) ? step : S.frames[g].step;
                                 const int remg = (ge - gc + gStep - 1) / gStep;
                                 const int keepChunks = (mode == 1) ? (remg + 1) / 2 : 0;
                                 const int newEnd = min(ge, gc + keepChunks * gStep);
@@ -821,14 +821,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                                         tk->pi[x] = (uint8_t)w_pi(wg);
                                     }
                                 }
-                                if (lane < g) tk->path[lane] = fMove;
+                                if (lane < g) tk->path[lane] = S.frames[lane].move;
                                 hdr1 = (uint32_t)g | ((uint32_t)gEven << 8);
                                 hdr2 = (uint32_t)newEnd | ((uint32_t)ge << 16);
                                 hdr3 = 0u;
                                 if (g == f) {
                                     end = newEnd;
-                                } else if (lane == g) {
-                                    fEnd = newEnd;
+                                } else if (lane == 0) {
+                                    S.frames[g].end = newEnd;
                                 }
                             }
                             if (lane == 0) {
@@ -899,7 +899,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                 const uint32_t wc = gather<NW>(w, c);
                 const int e = even + move_delta(wa, wb, wc);
                 const bool sat = valid && ((satMask >> e) & 1ull);
-                tChildren += (unsigned long long)nValid;
+                if (lane == 0) S.taskChildren += (unsigned long long)nValid;
                 const unsigned satBallot = __ballot_sync(kFull, sat);
                 if (satBallot) {
                     const int winner = __ffs(satBallot) - 1;
@@ -908,7 +908,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                     if (lane == 0) won = atomicCAS(&P.out[inst].state, kStateRunning, kStateFound) == kStateRunning;
                     won = __shfl_sync(kFull, won, 0);
                     if (won) {
-                        if (lane < f) P.out[inst].moves[lane] = fMove;
+                        if (lane < f) P.out[inst].moves[lane] = S.frames[lane].move;
                         if (lane == f) {
                             P.out[inst].moves[f] = wtr;
                             P.out[inst].depth = f + 1;
@@ -918,17 +918,29 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                     outcome = 1;
                     break;
                 }
-                bool adm = valid && ((expMask >> e) & 1ull);
-                if (adm) {
+                const bool probe = valid && ((expMask >> e) & 1ull);
+                const unsigned probing = __ballot_sync(kFull, probe);
+                uint32_t outc = 0u;
+                if (probe) {
                     uint64_t ck[KW];
 #pragma unroll
                     for (int q = 0; q < KW; ++q) ck[q] = key[q];
                     set_field<NW>(ck, a, w_spi(wc));
                     set_field<NW>(ck, b, w_spi(wa));
                     set_field<NW>(ck, c, w_spi(wb));
-                    adm = dedup_admit<KW>(P, generation, tag, ck, key_hash<KW>(ck, tag), (uint32_t)(f + 1), ls);
+                    outc = dedup_admit<KW>(P, generation, tag, ck, key_hash<KW>(ck, tag), (uint32_t)(f + 1));
                 }
-                pending = __ballot_sync(kFull, adm);
+                pending = __ballot_sync(kFull, outc & kAdmitted);
+                if (probing) {
+                    const unsigned ins = __ballot_sync(kFull, outc & kInserted);
+                    const unsigned full = __ballot_sync(kFull, outc & kWindowFull);
+                    if (lane == 0) {
+                        S.stats[kStatDedupProbes] += (unsigned)__popc(probing);
+                        S.stats[kStatDedupPruned] += (unsigned)__popc(probing & ~pending);
+                        S.stats[kStatDedupInserts] += (unsigned)__popc(ins);
+                        S.stats[kStatDedupFull] += (unsigned)__popc(full);
+                    }
+                }
                 continue;
             }
             // -------------------------------------------------------- descend
@@ -946,17 +958,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
                 const int t = chunk + l;
                 tr = __ldg(trip + ((rootOrder && f == 0) ? (int)__ldg(rootOrder + t) : t));
             }
-            if (lane == f) {
-                fCursor = cursor;
-                fEnd = end;
-                fPending = pending;
-                fChunk = chunk;
-                fEven = even;
-                fStep = sf.mode == 1 ? 1 : 32;
-                fMove = tr;
+            if (lane == 0) {
+                FrameRec<KW> &fr = S.frames[f];
+                fr.cursor = cursor;
+                fr.end = end;
+                fr.pending = pending;
+                fr.chunk = chunk;
+                fr.even = even;
+                fr.step = sf.mode == 1 ? 1 : 32;
+                fr.move = tr;
 #pragma unroll
-                for (int q = 0; q < KW; ++q) fKey[q] = key[q];
+                for (int q = 0; q < KW; ++q) fr.key[q] = key[q];
             }
+            __syncwarp();
             const uint32_t i = tri_i(tr), j = tri_j(tr), k = tri_k(tr);
             const uint32_t a = w_pi(gather<NW>(w, i));
             const uint32_t b = w_pi(gather<NW>(w, j));
@@ -984,17 +998,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
             ++f;
 #pragma unroll
             for (int h = 0; h < NW; ++h) S.words[f][h * 32 + lane] = w[h];
-            satMask = shfl64(ruleReg, f + 1);
-            expMask = shfl64(ruleReg, 16 + f + 1);
+            satMask = S.rules[f + 1];
+            expMask = S.rules[16 + f + 1];
             sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, (rootOrder && f == 0) ? 0 : P.sparse, S.tri);
             cursor = 0;
             end = sf.mode ? sf.np : T;
             pending = 0u;
-            ++tNodes;
+            if (lane == 0) ++S.taskNodes;
         }
         if (lane == 0) {
-            S.stats[kStatNodes] += tNodes;
-            S.stats[kStatChildren] += tChildren;
+            S.stats[kStatNodes] += S.taskNodes;
+            S.stats[kStatChildren] += S.taskChildren;
         }
         if (outcome == 2) {
             if (lane == 0) S.stats[kStatBusyCycles] += (unsigned long long)clock64();
@@ -1004,8 +1018,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
         // ---------------------------------------------------------------- finish task
         if (lane == 0) {
             S.stats[kStatBusyCycles] += (unsigned long long)clock64();
-            atomicAdd(&P.out[inst].nodes, tNodes);
-            atomicAdd(&P.out[inst].children, tChildren);
+            atomicAdd(&P.out[inst].nodes, S.taskNodes);
+            atomicAdd(&P.out[inst].children, S.taskChildren);
             const int prev = atomicSub(&P.out[inst].outstanding, 1);
             if (prev == 1) {
                 atomicCAS(&P.out[inst].state, kStateRunning, kStateNotFound);
@@ -1018,21 +1032,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 3 : 2) search_e
     }
 
     // ---------------------------------------------------------------- statistics
-    unsigned long long probes = ls.probes, pruned = ls.pruned, inserts = ls.inserts, full = ls.full;  // widen once
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        probes += __shfl_xor_sync(kFull, probes, o);
-        pruned += __shfl_xor_sync(kFull, pruned, o);
-        inserts += __shfl_xor_sync(kFull, inserts, o);
-        full += __shfl_xor_sync(kFull, full, o);
-    }
     if (lane == 0) {
         atomicAdd(&ctl->stats[kStatNodes], S.stats[kStatNodes]);
         atomicAdd(&ctl->stats[kStatChildren], S.stats[kStatChildren]);
-        atomicAdd(&ctl->stats[kStatDedupProbes], probes);
-        atomicAdd(&ctl->stats[kStatDedupPruned], pruned);
-        atomicAdd(&ctl->stats[kStatDedupInserts], inserts);
-        atomicAdd(&ctl->stats[kStatDedupFull], full);
+        atomicAdd(&ctl->stats[kStatDedupProbes], S.stats[kStatDedupProbes]);
+        atomicAdd(&ctl->stats[kStatDedupPruned], S.stats[kStatDedupPruned]);
+        atomicAdd(&ctl->stats[kStatDedupInserts], S.stats[kStatDedupInserts]);
+        atomicAdd(&ctl->stats[kStatDedupFull], S.stats[kStatDedupFull]);
         atomicAdd(&ctl->stats[kStatDonations], S.stats[kStatDonations]);
         atomicAdd(&ctl->stats[kStatTaskPops], S.stats[kStatTaskPops]);
         S.stats[kStatWarpCycles] += (unsigned long long)clock64();
