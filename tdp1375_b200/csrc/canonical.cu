@@ -17,12 +17,12 @@
 //    involution), the cycle's first position along pi (shared-memory atomicMin per cycle),
 //    label = rank of that first position among the cycles' first positions, orientation =
 //    more than one leap of pi^-1 positions around the cycle (atomicAdd per cycle), index of
-//    an oriented symbol along the cycle from the symbol at the cycle's first position;
-//  * the CRC32: CRC is linear over GF(2), so the hash of the row is the XOR over positions
-//    of (CRC of the position's 4 bytes) * x^(32 * words after it) mod P, plus the initial
-//    register carried over the whole row (the combination rule of zlib's crc32_combine),
-//    reduced across the warp with shuffles.
-// The best row so far stays in shared memory for the lexicographic tie-break.
+//    an oriented symbol along the cycle from the symbol at the cycle's first position.
+// Variants are built 32 at a time into a shared-memory block of rows; then the lanes switch to
+// variants and each computes its row's CRC32 from a byte table.  The least hash, ties broken
+// by the lexicographically least row, does not depend on the order the variants are
+// scanned in, so the groups give the reference's answer.  The best row so far stays in
+// shared memory.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,7 +48,10 @@ struct CanonArgs {
     int32_t *variant;
 };
 
+constexpr int kRowPitch = 65;  // floats per row: an odd pitch keeps variant-major reads off one bank
+
 struct WarpSmem {
+    float rows[32][kRowPitch];  // the current group of up to 32 variant rows
     float best[64];
     uint8_t spi[64], inv[64], leader[64], t[64], len[64];
     int firstPos[64], leaps[64], anchorT[64], count[64];
@@ -56,31 +59,13 @@ struct WarpSmem {
 
 __device__ __forceinline__ int mod_n(int x, int n) { return x >= n ? x - n : (x < 0 ? x + n : x); }
 
-// a * b mod P on reflected CRC-32 polynomials (bit 31 = x^0).
-__device__ __forceinline__ uint32_t gf2_mulmod(uint32_t a, uint32_t b) {
-    uint32_t p = 0u;
-    for (int k = 0; k < 32; ++k) {
-        if (a & 0x80000000u) p ^= b;
-        a <<= 1;
-        b = (b & 1u) ? (b >> 1) ^ kPoly : b >> 1;
-    }
-    return p;
-}
-
 __global__ void __launch_bounds__(kWarps * 32) canonical_kernel(const CanonArgs A) {
     __shared__ uint32_t crcTable[256];
-    __shared__ uint32_t xpow[kMaxN + 2];  // x^(32 m) mod P, m = 0..64
     __shared__ WarpSmem smem[kWarps];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
         uint32_t c = (uint32_t)i;
         for (int k = 0; k < 8; ++k) c = (c >> 1) ^ (kPoly & (0u - (c & 1u)));
         crcTable[i] = c;
-    }
-    __syncthreads();
-    for (int m = threadIdx.x; m <= kMaxN + 1; m += blockDim.x) {
-        uint32_t v = 0x80000000u;  // the polynomial 1
-        for (int k = 0; k < 4 * m; ++k) v = crcTable[v & 0xFFu] ^ (v >> 8);  // times x^8 per zero byte
-        xpow[m] = v;
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -146,104 +131,112 @@ __global__ void __launch_bounds__(kWarps * 32) canonical_kernel(const CanonArgs 
             }
         }
         __syncwarp();
-        const uint32_t initTerm = gf2_mulmod(xpow[n], 0xFFFFFFFFu);
         int32_t bestHash = INT32_MAX;
         int bestV = -1;
-        for (int v = 0; v < 2 * n; ++v) {
-            const int r = v >> 1;
-            const bool mirror = v & 1;
-            S.firstPos[lane] = 127;
-            S.firstPos[lane + 32] = 127;
-            S.leaps[lane] = 0;
-            S.leaps[lane + 32] = 0;
-            __syncwarp();
-            int cid[2], tS[2], L[2];
-            bool act[2];
+        for (int group = 0; group < 2 * n; group += 32) {
+            const int nv = min(32, 2 * n - group);
+            for (int k = 0; k < nv; ++k) {
+                const int v = group + k;
+                const int r = v >> 1;
+                const bool mirror = v & 1;
+                S.firstPos[lane] = 127;
+                S.firstPos[lane + 32] = 127;
+                S.leaps[lane] = 0;
+                S.leaps[lane + 32] = 0;
+                __syncwarp();
+                int cid[2], tS[2], L[2];
+                bool act[2];
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int p = lane + 32 * h;
-                act[h] = p < n;
-                cid[h] = 0, tS[h] = 0, L[h] = 1;
-                if (act[h]) {
-                    const int s = mod_n(r + p, n);
-                    int succ;
-                    if (!mirror) {
-                        succ = S.spi[s];
-                        cid[h] = S.leader[s];
-                        tS[h] = S.t[s];
-                        L[h] = S.len[s];
-                    } else {
-                        // c(x) = symbol at pi position n-1-pos(x); m(x) = c(spi^-1(c(x)))
-                        const int cs = mod_n(r + (n - 1 - p), n);
-                        const int pp = mod_n((int)S.inv[cs] - r, n);
-                        succ = mod_n(r + (n - 1 - pp), n);
-                        cid[h] = S.leader[cs];
-                        L[h] = S.len[cs];
-                        tS[h] = S.t[cs] == 0 ? 0 : L[h] - S.t[cs];  // m runs spi's cycle backwards
-                    }
-                    atomicMin(&S.firstPos[cid[h]], p);
-                    // leap of pi^-1 positions: n-1-pos(s) > n-1-pos(succ) <=> pos(s) < pos(succ)
-                    if (p < mod_n(succ - r, n)) atomicAdd(&S.leaps[cid[h]], 1);
-                }
-            }
-            __syncwarp();
-            bool isFirst[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                isFirst[h] = act[h] && S.firstPos[cid[h]] == lane + 32 * h;
-                if (isFirst[h]) S.anchorT[cid[h]] = tS[h];
-            }
-            const uint64_t firsts = (uint64_t)__ballot_sync(kFull, isFirst[0]) |
-                                    ((uint64_t)__ballot_sync(kFull, isFirst[1]) << 32);
-            __syncwarp();
-            float value[2];
-            uint32_t crc = 0u;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                value[h] = 0.f;
-                if (act[h]) {
+                for (int h = 0; h < 2; ++h) {
                     const int p = lane + 32 * h;
-                    const int fp = S.firstPos[cid[h]];
-                    const uint64_t upTo = (fp >= 63) ? ~0ull : ((2ull << fp) - 1ull);
-                    const int label = __popcll(firsts & upTo);
-                    const bool oriented = S.leaps[cid[h]] > 1;
-                    int idx = tS[h] - S.anchorT[cid[h]];
-                    if (idx < 0) idx += L[h];
-                    const float fl = __int2float_rn(label);
-                    value[h] = oriented ? __fadd_rn(fl, __fdiv_rn(__int2float_rn(idx + 1), 100.0f)) : fl;
-                    // CRC register of this position's 4 big-endian bytes from zero, carried over
-                    // the words that follow it
-                    const uint32_t bits = __float_as_uint(value[h]);
-                    uint32_t w = 0u;
+                    act[h] = p < n;
+                    cid[h] = 0, tS[h] = 0, L[h] = 1;
+                    if (act[h]) {
+                        const int s = mod_n(r + p, n);
+                        int succ;
+                        if (!mirror) {
+                            succ = S.spi[s];
+                            cid[h] = S.leader[s];
+                            tS[h] = S.t[s];
+                            L[h] = S.len[s];
+                        } else {
+                            // c(x) = symbol at pi position n-1-pos(x); m(x) = c(spi^-1(c(x)))
+                            const int cs = mod_n(r + (n - 1 - p), n);
+                            const int pp = mod_n((int)S.inv[cs] - r, n);
+                            succ = mod_n(r + (n - 1 - pp), n);
+                            cid[h] = S.leader[cs];
+                            L[h] = S.len[cs];
+                            tS[h] = S.t[cs] == 0 ? 0 : L[h] - S.t[cs];  // m runs spi's cycle backwards
+                        }
+                        atomicMin(&S.firstPos[cid[h]], p);
+                        // leap of pi^-1 positions: n-1-pos(s) > n-1-pos(succ) <=> pos(s) < pos(succ)
+                        if (p < mod_n(succ - r, n)) atomicAdd(&S.leaps[cid[h]], 1);
+                    }
+                }
+                __syncwarp();
+                bool isFirst[2];
 #pragma unroll
-                    for (int b = 3; b >= 0; --b) w = crcTable[(w ^ (bits >> (8 * b))) & 0xFFu] ^ (w >> 8);
-                    crc ^= gf2_mulmod(xpow[n - 1 - p], w);
+                for (int h = 0; h < 2; ++h) {
+                    isFirst[h] = act[h] && S.firstPos[cid[h]] == lane + 32 * h;
+                    if (isFirst[h]) S.anchorT[cid[h]] = tS[h];
+                }
+                const uint64_t firsts = (uint64_t)__ballot_sync(kFull, isFirst[0]) |
+                                        ((uint64_t)__ballot_sync(kFull, isFirst[1]) << 32);
+                __syncwarp();
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    if (act[h]) {
+                        const int fp = S.firstPos[cid[h]];
+                        const uint64_t upTo = (fp >= 63) ? ~0ull : ((2ull << fp) - 1ull);
+                        const int label = __popcll(firsts & upTo);
+                        const bool oriented = S.leaps[cid[h]] > 1;
+                        int idx = tS[h] - S.anchorT[cid[h]];
+                        if (idx < 0) idx += L[h];
+                        const float fl = __int2float_rn(label);
+                        S.rows[k][lane + 32 * h] =
+                            oriented ? __fadd_rn(fl, __fdiv_rn(__int2float_rn(idx + 1), 100.0f)) : fl;
+                    }
+                }
+                __syncwarp();
+            }
+            // lanes = variants of the group: CRC32 of the row's big-endian float bytes
+            int32_t h = INT32_MAX;
+            if (lane < nv) {
+                uint32_t crc = 0xFFFFFFFFu;
+                for (int i = 0; i < n; ++i) {
+                    const uint32_t bits = __float_as_uint(S.rows[lane][i]);
+#pragma unroll
+                    for (int b = 3; b >= 0; --b) crc = crcTable[(crc ^ (bits >> (8 * b))) & 0xFFu] ^ (crc >> 8);
+                }
+                h = (int32_t)(crc ^ 0xFFFFFFFFu);
+            }
+            const int32_t m = __reduce_min_sync(kFull, h);
+            const unsigned cand = __ballot_sync(kFull, lane < nv && h == m);
+            // Configuration.getCanonical: the least hash, ties by Arrays.compare
+            if (lane == 0 && m <= bestHash) {
+                unsigned c = cand;
+                while (c) {
+                    const int w = __ffs(c) - 1;
+                    c &= c - 1u;
+                    bool take = bestV < 0 || m < bestHash;
+                    if (!take) {
+                        for (int i = 0; i < n; ++i) {
+                            const float a = S.rows[w][i], b = S.best[i];
+                            if (a != b) {
+                                take = a < b;
+                                break;
+                            }
+                        }
+                    }
+                    if (take) {
+                        bestHash = m;
+                        bestV = group + w;
+                        for (int i = 0; i < n; ++i) S.best[i] = S.rows[w][i];
+                    }
                 }
             }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) crc ^= __shfl_xor_sync(kFull, crc, o);
-            const int32_t hv = (int32_t)((crc ^ initTerm) ^ 0xFFFFFFFFu);
-            // Configuration.getCanonical: strictly smaller hash, or equal hash and a
-            // lexicographically smaller row (Arrays.compare)
-            bool take = bestV < 0 || hv < bestHash;
-            if (!take && hv == bestHash) {
-                const bool d0 = act[0] && value[0] != S.best[lane];
-                const bool d1 = act[1] && value[1] != S.best[lane + 32];
-                const uint64_t diff = (uint64_t)__ballot_sync(kFull, d0) | ((uint64_t)__ballot_sync(kFull, d1) << 32);
-                if (diff) {
-                    const int q = __ffsll((long long)diff) - 1;
-                    const float v0 = __shfl_sync(kFull, value[0], q & 31);
-                    const float v1 = __shfl_sync(kFull, value[1], q & 31);
-                    take = (q < 32 ? v0 : v1) < S.best[q];
-                }
-            }
-            __syncwarp();
-            if (take) {
-                bestHash = hv;
-                bestV = v;
-                if (act[0]) S.best[lane] = value[0];
-                if (act[1]) S.best[lane + 32] = value[1];
-            }
+            bestHash = __shfl_sync(kFull, bestHash, 0);
+            bestV = __shfl_sync(kFull, bestV, 0);
             __syncwarp();
         }
         dst[lane] = lane < n ? S.best[lane] : 0.f;
