@@ -262,7 +262,12 @@ __device__ __forceinline__ uint32_t dedup_admit(const EngineParams &P, uint32_t 
         }
     }
     const int freeSlot = freeMask ? (__ffs(freeMask) - 1) : -1;
-    const uint32_t freeTag = freeSlot >= 0 ? tags[freeSlot] : 0u;
+    // an unrolled select keeps the tags in registers (a dynamic index would put them in
+    // local memory on every probe)
+    uint32_t freeTag = 0u;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        if (q == freeSlot) freeTag = tags[q];
     if (freeSlot >= 0) {
         DedupEntry<KW> *e = &table[base + freeSlot];
         if (atomicCAS(tagArr + base + freeSlot, freeTag, kTagWriting) == freeTag) {
