@@ -189,11 +189,10 @@ def measured_hbm():
 
 
 def algorithmic_bytes(stats, instances: int) -> float:
-    """Bytes the search must move per launch: every transposition-table probe reads its
-    window's tag sector (32 B) and one 32 B entry, every insert writes a 32 B entry and a
-    4 B tag, every donated task is written and read once (2 x 208 B), every instance is read
-    (144 B) and written (96 B)."""
-    return 64.0 * stats.dedup_probes + 36.0 * stats.dedup_inserts + 416.0 * stats.donations + 240.0 * instances
+    """Bytes the search must move per launch: every transposition-table probe touches a window
+    of 8 entries (8 sectors of 32 B), every insert writes one 32 B entry, every donated task
+    is written and read once (2 x 208 B), every instance is read (144 B) and written (96 B)."""
+    return 256.0 * stats.dedup_probes + 32.0 * stats.dedup_inserts + 416.0 * stats.donations + 240.0 * instances
 
 
 def run_ours(args):

@@ -106,13 +106,11 @@ constexpr uint32_t kMaxGeneration = 4094;  // generation 4095 would collide with
 constexpr int kInstanceBits = 20;          // up to 1,048,576 instances per launch
 
 // Transposition-table entry.  key = spi packed 5 bits/symbol, 12 per word (n <= 32) or
-// 6 bits/symbol, 10 per word (n <= 63).  Its tag (generation << 20 | instance) lives at the
-// same index of a separate tag array, so the 8 tags of a probe window share one 32-byte
-// sector.
+// 6 bits/symbol, 10 per word (n <= 63).  tag = generation << 20 | instance.
 template <int KW>
 struct alignas(KW == 3 ? 32 : 64) DedupEntry {
+    uint32_t tag;
     uint32_t depth;
-    uint32_t pad;
     uint64_t key[KW];
 };
 
@@ -123,8 +121,7 @@ struct EngineParams {
     int pollInterval;
     const RuleTable *rules;
     const uint32_t *triples;  // lexicographic (i,j,k) per n at offset combinations4(n)
-    void *table;              // DedupEntry<KW>[entries]
-    uint32_t *tags;           // tag of each entry
+    void *table;
     uint32_t tableMask;       // entries - 1 (entries of this launch's layout)
     const uint32_t *generation;  // device word: this launch's table generation (1..4094)
     uint32_t *doneBits;

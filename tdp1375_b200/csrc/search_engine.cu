@@ -95,9 +95,7 @@ SearchSlot::SearchSlot(int device, int64_t queueBytesBudget, int dedupTableSize)
 
     tableEntries32_ = round_pow2((uint64_t)std::max(dedupTableSize, 1024));
     check(cudaMalloc(&dTable_, (size_t)tableEntries32_ * 32), "cudaMalloc(dedup table)");
-    check(cudaMalloc(&dTags_, (size_t)tableEntries32_ * 4), "cudaMalloc(dedup tags)");
     check(cudaMemset(dTable_, 0, (size_t)tableEntries32_ * 32), "cudaMemset(dedup table)");
-    check(cudaMemset(dTags_, 0, (size_t)tableEntries32_ * 4), "cudaMemset(dedup tags)");
     // One mailbox per warp of the largest grid this slot launches, and an idle-warp ring with
     // at least as many slots.  The queue budget of the reference (bytes for node queues)
     // bounds the mailbox area; the default budgets leave room for every resident warp.
@@ -125,7 +123,6 @@ SearchSlot::~SearchSlot() {
     if (stream_) cudaStreamSynchronize(stream_);
     if (cancelStream_) cudaStreamSynchronize(cancelStream_);
     cudaFree(dTable_);
-    cudaFree(dTags_);
     cudaFree(dMail_);
     cudaFree(dRing_);
     cudaFree(dCtl_);
@@ -299,7 +296,6 @@ void SearchSlot::launchClass(int cls, int offset, int count) {
     P.rules = dRules_;
     P.triples = triples_;
     P.table = dTable_;
-    P.tags = dTags_;
     P.tableMask = (cls == 0 ? tableEntries32_ : tableEntries32_ / 2) - 1u;
     P.generation = dGen_;
     P.doneBits = dDone_;
@@ -376,8 +372,7 @@ int SearchSlot::runStaged(std::string &err) {
         const int n = cls == 0 ? countSmall_ : count_ - countSmall_;
         if (n <= 0) continue;
         if (generation_ >= kMaxGeneration || cls != lastLayout_) {
-            // the tags alone decide which entries are live: clearing them empties the table
-            check(cudaMemsetAsync(dTags_, 0, (size_t)tableEntries32_ * 4, stream_), "clear dedup tags");
+            check(cudaMemsetAsync(dTable_, 0, (size_t)tableEntries32_ * 32, stream_), "clear dedup table");
             generation_ = 0;
             lastLayout_ = cls;
         }

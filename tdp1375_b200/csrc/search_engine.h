@@ -80,7 +80,6 @@ private:
 
     const uint32_t *triples_ = nullptr;
     void *dTable_ = nullptr;
-    uint32_t *dTags_ = nullptr;
     uint32_t tableEntries32_ = 0;
     uint32_t generation_ = 0;
     int lastLayout_ = -1;

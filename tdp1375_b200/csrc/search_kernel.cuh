@@ -63,14 +63,6 @@ __device__ __forceinline__ int ld_relaxed_s32(const int *p) {
     asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ uint4 ld_relaxed_v4(const uint32_t *p) {
-    uint4 v;
-    asm volatile("ld.relaxed.gpu.global.v4.u32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                 : "l"(p)
-                 : "memory");
-    return v;
-}
 __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
     uint32_t v;
     asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -213,14 +205,13 @@ template <int KW>
 __device__ __forceinline__ uint32_t dedup_admit(const EngineParams &P, uint32_t generation, uint32_t tag,
                                             const uint64_t (&key)[KW], uint64_t h, uint32_t depth) {
     auto *table = reinterpret_cast<DedupEntry<KW> *>(P.table);
-    uint32_t *tagArr = P.tags;
     const uint32_t base = (uint32_t)(h >> 24) & P.tableMask & ~7u;
-    // The window's eight tags are one 32-byte sector: two relaxed vector loads (one round
-    // trip; each 32-bit tag is read single-copy atomically).  Only when a tag matches does the
+    // Eight independent relaxed tag loads (one round trip); only when a tag matches does the
     // lane pay an acquire fence before reading keys, which pairs with the release store that
-    // published the entry.
-    const uint4 t0 = ld_relaxed_v4(tagArr + base), t1 = ld_relaxed_v4(tagArr + base + 4);
-    const uint32_t tags[8] = {t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w};
+    // published the entry.  (Eight acquire loads would serialise into eight round trips.)
+    uint32_t tags[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) tags[q] = ld_relaxed_u32(&table[base + q].tag);
     bool anyMatch = false;
 #pragma unroll
     for (int q = 0; q < 8; ++q) anyMatch |= (tags[q] == tag);
@@ -270,11 +261,11 @@ __device__ __forceinline__ uint32_t dedup_admit(const EngineParams &P, uint32_t 
         if (q == freeSlot) freeTag = tags[q];
     if (freeSlot >= 0) {
         DedupEntry<KW> *e = &table[base + freeSlot];
-        if (atomicCAS(tagArr + base + freeSlot, freeTag, kTagWriting) == freeTag) {
+        if (atomicCAS(&e->tag, freeTag, kTagWriting) == freeTag) {
             e->depth = depth;
 #pragma unroll
             for (int kq = 0; kq < KW; ++kq) __stcg(&e->key[kq], key[kq]);
-            st_release_u32(tagArr + base + freeSlot, tag);  // orders the depth and key stores before it
+            st_release_u32(&e->tag, tag);  // the release orders the depth and key stores before it
             return kAdmitted | kInserted;
         }
         return kAdmitted;
