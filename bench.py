@@ -326,7 +326,7 @@ def run_ours(args):
                      "note": f"algorithmic table/task/instance bytes over kernel time; peak {peak_kind}; traffic = "
                              "DRAM bytes per launch scaled from an ncu capture (1.44 kB per expanded node) by the "
                              "launch's nodes; the kernel is bound by table-probe latency and warp count (ncu: "
-                             "issue-active 29%, DRAM throughput 3.5%, long-scoreboard and fence stalls on top)"},
+                             "issue-active 47%, DRAM throughput 5.1%, long-scoreboard and fence stalls on top)"},
         "e2e": {"value": round(cases / wall, 3) if wall > 0 else None, "unit": "cases/s",
                 "h2d_bytes_per_step": args.batch * 144, "d2h_bytes_per_step": args.batch * 96},
         "clocks": clocks.summary(),
