@@ -6,7 +6,8 @@ the oracle's restatement of the CUDA rule (oracle/tdp_oracle.cpp) with the trans
 table and the verdict-preserving tight bound.  Cases with m = 8 are left out: an exhaustive
 m = 8 negative takes tens of millions of nodes on one core.  A verdict of -2 means the node
 limit was hit (the case is not used by the tests).  Runs on all cores with a spawn pool:
-    python tests/golden/make_verdicts_config2.py [scan] [node_limit]
+    python tests/golden/make_verdicts_config2.py [scan] [node_limit] [start]
+With start > 0 the cases [start, start + scan) are solved and merged into the existing file.
 """
 from __future__ import annotations
 
@@ -34,13 +35,20 @@ def solve(args):
 def main():
     scan = int(sys.argv[1]) if len(sys.argv) > 1 else 6250
     node_limit = int(sys.argv[2]) if len(sys.argv) > 2 else 20_000_000
+    start = int(sys.argv[3]) if len(sys.argv) > 3 else 0
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "verdicts_config2.json")
     ctx = mp.get_context("spawn")
     with ctx.Pool(os.cpu_count()) as pool:
-        rows = [r for r in pool.map(solve, [(c, node_limit) for c in range(scan)], chunksize=4) if r is not None]
-    data = {"config": 2, "min_rate": "float32(2)/float32(1.375)", "node_limit": node_limit, "scanned": scan,
+        rows = [r for r in pool.map(solve, [(c, node_limit) for c in range(start, start + scan)], chunksize=4)
+                if r is not None]
+    if start > 0:
+        old = json.load(open(path))
+        if old["scanned"] != start or old["node_limit"] != node_limit:
+            raise SystemExit("the existing file must cover exactly [0, start) with the same node limit")
+        rows = old["cases"] + rows
+    data = {"config": 2, "min_rate": "float32(2)/float32(1.375)", "node_limit": node_limit, "scanned": start + scan,
             "rule": "sorting_search.cu:321-362 (float32), full sorting, depth 11, transposition table and tight bound",
             "cases": rows}
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "verdicts_config2.json")
     with open(path, "w") as fh:
         json.dump(data, fh, separators=(",", ":"))
     vals = [r["full11"] for r in rows]
