@@ -68,6 +68,8 @@ int tdp_cancel(int slot);
  * (the reference's order is arbitrary), and returns the total number of hits (< 0: error). */
 int64_t tdp_pi_filter(const uint8_t *cycle, int cycle_len, const uint8_t *oriented_triple, int triple_len, int n,
                       int skip_2move_check, uint8_t *out, int64_t max_rows);
+/* Device time in ms (CUDA events around its kernels) of this thread's last tdp_pi_filter call. */
+double tdp_pi_filter_last_kernel_ms(void);
 
 /* ---- batched search (no counterpart in the reference; one persistent launch over many
  *      instances with device-side admission) ---------------------------------------- */
@@ -112,6 +114,9 @@ typedef struct tdp_stats {
     int32_t launches;
     uint64_t busy_warp_cycles; /* SM cycles warps spent holding a task, summed over warps */
     uint64_t warp_cycles;      /* SM cycles from each warp's start to its exit, summed */
+    uint64_t dedup_replaced;   /* inserts that overwrote a live entry of a full probe window */
+    uint64_t table_atomics;    /* table atomics issued: entry claims and best-depth updates */
+    uint64_t commute_skips;    /* children skipped by the partial-order reduction (commute) */
 } tdp_stats;
 
 /* Statistics of the last search/batch run on the slot. */
@@ -129,6 +134,19 @@ typedef struct tdp_engine_config {
     int32_t warps_per_instance; /* 0 = admit instances while any warp is free; w > 0 = at most
                                    (grid warps / w) instances in flight, the other warps join them
                                    through work donation (bounds the live transposition-table load) */
+    int32_t table_replacement;  /* what a full 8-entry probe window does with a new state:
+                                   0 = admit it without recording, as sorting_search.cu:291-297;
+                                   1 = overwrite the deepest entry if it is at least as deep;
+                                   2 = overwrite the oldest entry; 3 = overwrite the deepest
+                                   entry, the oldest among equally deep ones.  Verdicts are the
+                                   same under every policy; the default is 2 (on a table far
+                                   smaller than a search's states, recency keeps the duplicates
+                                   that nearby subtrees produce). */
+    int32_t commute;            /* 1 (default) = partial-order reduction: a child move on symbols
+                                   disjoint from the move that reached the node is skipped when the
+                                   two moves could also be made in the other order and the child's
+                                   smallest symbol is the smaller (that order reaches the same state
+                                   at the same depth); 0 = every child.  Verdicts are the same. */
     int32_t reserved;
 } tdp_engine_config;
 
@@ -203,19 +221,31 @@ int tdp_set_order_model(int slot, const uint16_t *w1, const float *b1, const uin
 int tdp_enable_order_model(int slot, int enable);
 
 /* ---- allocation-free permutation filter (no counterpart in the reference) ------------
- * For callers that must not allocate device memory: code running while a CUDA stream is
- * being captured, host runtimes whose own allocator owns the whole device heap, and
- * real-time hosts that forbid allocation once they are running.  It is the filter of
- * tdp_pi_filter, but it calls no cudaMalloc/cudaFree: its scratch is a static 156 KB device
- * array inside this library (held on every GPU that loads it until the process exits), and
- * rows go to out_device, a DEVICE buffer of max_rows * n bytes owned by the caller.
- * Limit: n <= 12 ((n-1)! <= 11! candidates); larger n returns TDP_ERR_ARGUMENT.  Work runs
- * on `stream` (a cudaStream_t, may be null); the call returns after it with the total number
- * of hits.  The first call on a device looks up the scratch address (cudaGetSymbolAddress):
- * make that first call outside any stream capture.  All calls share the scratch, so calls
- * that overlap on the GPU (different streams or threads at once) race; serialise them. */
+ * The same filter as tdp_pi_filter for hosts that must not call cudaMalloc: a JVM or
+ * database process whose own pool allocator already owns the device heap (a second
+ * allocator would fragment it or fail), and real-time services that allocate everything at
+ * start-up and may not allocate, nor take the allocator's locks, once they serve requests.
+ * It calls no cudaMalloc, cudaFree or allocating library routine.  Its scratch is a static
+ * 156 KB device array inside this library, which every GPU that loads the library holds
+ * until the process exits; the caller passes the inputs in host memory and out_device, a
+ * DEVICE buffer of max_rows * n bytes that it owns.  Limit: n <= 12, i.e. (n-1)! <= 11!
+ * candidates; a larger n returns TDP_ERR_ARGUMENT.  The work runs on `stream` (a
+ * cudaStream_t, may be null) and the call returns when it is done, with the total number
+ * of hits (rows beyond max_rows are counted but not written).  The first call on a device
+ * (and the first after that device's context was reset) looks up the array's device
+ * address with cudaGetSymbolAddress; make that first call before any stream capture.  All
+ * calls share the one array and it keeps the last call's contents, so calls that overlap
+ * on the GPU (other streams or threads at the same time) race: serialise them. */
 int64_t tdp_pi_filter_noalloc(const uint8_t *cycle, int cycle_len, const uint8_t *oriented_triple, int triple_len,
                               int n, int skip_2move_check, uint8_t *out_device, int64_t max_rows, void *stream);
+
+/* ---- measurement helper (no counterpart in the reference) ---------------------------
+ * Throughput of returning 32-bit atomics (atomicCAS if use_cas, else atomicAdd) at random
+ * 32-byte entries of a fresh device buffer of `entries` entries (a power of two), on the
+ * current device: with entries * 32 bytes below the L2 size this is the L2 atomic roof that
+ * bounds transposition-table claims.  Allocates and frees its buffer. */
+int tdp_measure_atomics(int64_t entries, int use_cas, int iters, double *atomics_per_s);
+const char *tdp_measure_last_error(void);
 
 #ifdef __cplusplus
 }

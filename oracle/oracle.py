@@ -67,12 +67,15 @@ def rule_eval(n, initial_even, min_rate, max_depth, full, even, depth) -> int:
     return lib().oracle_rule_eval(n, initial_even, ctypes.c_float(min_rate), max_depth, 1 if full else 0, even, depth)
 
 
-def search_gpu_rule(pi, spi, initial_even, min_rate, max_depth, full, dedup=True, tight=False, node_limit=0):
-    """Returns (status, positions[[i,j,k]...], (expanded, children)); status 1/0, -2 node limit."""
+def search_gpu_rule(pi, spi, initial_even, min_rate, max_depth, full, dedup=True, tight=False, node_limit=0,
+                    commute=False):
+    """Returns (status, positions[[i,j,k]...], (expanded, children)); status 1/0, -2 node limit.
+    commute: skip children that commute with the incoming move in the other order (the
+    engine's partial-order reduction, restated for cross-checking)."""
     pos = (ctypes.c_int * 48)()
     depth = ctypes.c_int(0)
     stats = (ctypes.c_uint64 * 2)()
-    mode = (1 if dedup else 0) | (2 if tight else 0)
+    mode = (1 if dedup else 0) | (2 if tight else 0) | (4 if commute else 0)
     st = lib().oracle_search_gpu_rule(_u8(pi), _u8(spi), len(pi), initial_even, ctypes.c_float(min_rate), max_depth,
                                       1 if full else 0, mode, node_limit, pos, ctypes.byref(depth), stats)
     moves = [[pos[3 * d], pos[3 * d + 1], pos[3 * d + 2]] for d in range(depth.value)]

@@ -14,13 +14,14 @@ import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_ref", "libtdp_ref.so")
+LIB_DEBUG = os.path.join(HERE, "_ref", "libtdp_ref_g.so")  # device code unoptimised (make ref-debug)
 
 NOT_FOUND, FOUND, TIMED_OUT, OVERFLOW, ERROR = 0, 1, 2, 3, -1
 STATUS_NAME = {NOT_FOUND: "not_found", FOUND: "found", TIMED_OUT: "timeout", OVERFLOW: "overflow", ERROR: "error"}
 
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _i32p = ctypes.POINTER(ctypes.c_int32)
-_lib = None
+_libs = {}
 
 
 def build(reference_root: str) -> str:
@@ -29,16 +30,18 @@ def build(reference_root: str) -> str:
     return LIB
 
 
-def available() -> bool:
-    return os.path.exists(LIB)
+def available(debug: bool = False) -> bool:
+    return os.path.exists(LIB_DEBUG if debug else LIB)
 
 
-def lib() -> ctypes.CDLL:
-    global _lib
-    if _lib is None:
-        if not available():
-            raise RuntimeError(f"{LIB} is not built (make -C oracle ref REF=<reference checkout>)")
-        L = ctypes.CDLL(LIB)
+def lib(debug: bool = False) -> ctypes.CDLL:
+    """The optimised build, or with debug=True the build whose device code is unoptimised
+    (make -C oracle ref-debug); both can be loaded in one process."""
+    path = LIB_DEBUG if debug else LIB
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is not built (make -C oracle ref ref-debug REF=<reference checkout>)")
+        L = ctypes.CDLL(path)
         L.ref_last_error.restype = ctypes.c_char_p
         L.ref_init.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_int]
         L.ref_search.argtypes = [ctypes.c_int, _u8p, _u8p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
@@ -46,12 +49,12 @@ def lib() -> ctypes.CDLL:
         L.ref_pi_filter.restype = ctypes.c_longlong
         L.ref_pi_filter.argtypes = [_u8p, ctypes.c_int, _u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _u8p,
                                     ctypes.c_longlong]
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
-def last_error() -> str:
-    return lib().ref_last_error().decode()
+def last_error(debug: bool = False) -> str:
+    return lib(debug).ref_last_error().decode()
 
 
 def _u8(seq):
@@ -85,13 +88,13 @@ def search(pi, spi, initial_even, min_rate, max_depth, full, timeout_s=60.0, slo
     return st, moves, ms.value
 
 
-def pi_filter(cycle, triple, n, skip_2move, max_rows=1 << 20):
+def pi_filter(cycle, triple, n, skip_2move, max_rows=1 << 20, debug=False):
     """performGpuPiFilter.  Returns the hit rows (bytes of length n) sorted, so that runs with
     the reference's arbitrary row order compare as sets."""
     out = (ctypes.c_uint8 * max(1, max_rows * n))()
-    rows = lib().ref_pi_filter(_u8(cycle), len(cycle), _u8(triple), len(triple), n, 1 if skip_2move else 0, out,
-                               max_rows)
+    rows = lib(debug).ref_pi_filter(_u8(cycle), len(cycle), _u8(triple), len(triple), n, 1 if skip_2move else 0, out,
+                                    max_rows)
     if rows < 0:
-        raise RuntimeError(last_error())
+        raise RuntimeError(last_error(debug))
     raw = bytes(out)[: min(rows, max_rows) * n]
     return sorted(raw[r * n:(r + 1) * n] for r in range(min(rows, max_rows)))

@@ -34,6 +34,7 @@
 //   oracle_pi_filter              pi_filter.cu:38-154 (factoradic rank order, the
 //                                 three predicates), CommonOperations.java:167-182,
 //                                 406-445
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -143,10 +144,40 @@ bool tight_reach(const Rule &r, int even, int depth) {
     return false;
 }
 
+// Partial-order reduction (not in the reference; verdict-preserving, used by the engine's
+// `commute` option).  At a node N reached by the move (x y z) at positions I<J<K of its
+// parent P, the child (a b c) at positions i<j<k of N is skipped when {a,b,c} and {x,y,z}
+// are disjoint, (a b c) is also a move at P (a, b, c in cyclic order there), (x y z) is a
+// move after it, and the sorted triple (a,b,c) is smaller than the sorted (x,y,z): then
+// P.(a b c).(x y z) reaches the same state (disjoint 3-cycles commute) through the kept
+// order.  Positions in P follow from N's by the inverse block swap of (I,J,K).
+bool cyclic3(int pa, int pb, int pc) { return ((pa > pb) + (pb > pc) + (pc > pa)) <= 1; }
+
+bool por_skip(const uint8_t *pi, int I, int J, int K, int i, int j, int k) {
+    const int a = pi[i], b = pi[j], c = pi[k];
+    const int y = pi[I], x = pi[I + K - J], z = pi[K];
+    if (a == x || a == y || a == z || b == x || b == y || b == z || c == x || c == y || c == z) return false;
+    const int pa = src_index(i, I, J, K), pb = src_index(j, I, J, K), pc = src_index(k, I, J, K);
+    if (!cyclic3(pa, pb, pc)) return false;
+    int q[3] = {pa, pb, pc};
+    std::sort(q, q + 3);
+    auto fwd = [&](int p) {
+        if (p >= q[0] && p < q[1]) return p + (q[2] - q[1]);
+        if (p >= q[1] && p < q[2]) return p - (q[1] - q[0]);
+        return p;
+    };
+    if (!cyclic3(fwd(I), fwd(J), fwd(K))) return false;
+    int me[3] = {a, b, c}, in[3] = {x, y, z};
+    std::sort(me, me + 3);
+    std::sort(in, in + 3);
+    return std::lexicographical_compare(me, me + 3, in, in + 3);
+}
+
 struct GpuRuleDfs {
     Rule rule;
     bool useDedup;
     bool tight = false;
+    bool por = false;
     std::unordered_map<std::string, int> memo;
     uint64_t expanded = 0;
     uint64_t children = 0;
@@ -197,6 +228,8 @@ struct GpuRuleDfs {
                     }
                     if (childDepth < rule.maxDepth && gpu_reach(rule, even, childDepth) &&
                         (!tight || tight_reach(rule, even, childDepth)) &&
+                        !(por && depth > 0 &&
+                          por_skip(pi, path[depth - 1][0], path[depth - 1][1], path[depth - 1][2], i, j, k)) &&
                         admit(childSpi, childDepth)) {
                         apply_block_swap(pi, n, i, j, k, childPi);
                         if (expand(childSpi, childPi, childDepth)) return true;
@@ -331,6 +364,7 @@ int oracle_search_gpu_rule(const uint8_t *pi, const uint8_t *spi, int n, int ini
     dfs.rule = Rule{n, initialEven, maxDepth, minRate, fullSorting};
     dfs.useDedup = (useDedup & 1) != 0;
     dfs.tight = (useDedup & 2) != 0;
+    dfs.por = (useDedup & 4) != 0;
     dfs.nodeLimit = nodeLimit;
     uint8_t s[kMaxN + 1], p[kMaxN + 1];
     std::memcpy(s, spi, n);

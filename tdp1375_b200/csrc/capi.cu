@@ -19,6 +19,12 @@
 #include "pi_filter.h"
 #include "search_engine.h"
 
+// The ABI structs have fixed sizes (the ctypes mirror in tdp1375_b200/native.py checks them too).
+static_assert(sizeof(tdp_instance) == 136, "tdp_instance layout");
+static_assert(sizeof(tdp_result) == 208, "tdp_result layout");
+static_assert(sizeof(tdp_stats) == 120, "tdp_stats layout");
+static_assert(sizeof(tdp_engine_config) == 48, "tdp_engine_config layout");
+
 namespace {
 
 thread_local std::string gLastError;
@@ -208,11 +214,14 @@ int tdp_set_engine_config(int slot, const tdp_engine_config *cfg) {
     auto s = get_slot(slot);
     if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
     if (!cfg || cfg->poll_interval <= 0 || cfg->time_limit_s <= 0 || cfg->blocks_per_sm < 0 ||
-        cfg->warps_per_instance < 0 || cfg->sparse_enumeration < 0 || cfg->sparse_enumeration > 2)
+        cfg->warps_per_instance < 0 || cfg->sparse_enumeration < 0 || cfg->sparse_enumeration > 2 ||
+        cfg->table_replacement < 0 || cfg->table_replacement > 3 || cfg->commute < 0 || cfg->commute > 1)
         return fail(TDP_ERR_ARGUMENT, "tdp_set_engine_config: invalid configuration");
     s->setConfig(*cfg);
     return 0;
 }
+
+double tdp_pi_filter_last_kernel_ms(void) { return tdp::gLastFilterKernelMs; }
 
 int64_t tdp_pi_filter(const uint8_t *cycle, int cycle_len, const uint8_t *oriented_triple, int triple_len, int n,
                       int skip_2move_check, uint8_t *out, int64_t max_rows) {

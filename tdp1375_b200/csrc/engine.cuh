@@ -68,6 +68,9 @@ enum EngineStat : int {
     kStatTaskPops,
     kStatBusyCycles,  // SM cycles warps spent holding a task
     kStatWarpCycles,  // SM cycles of every warp from start to exit
+    kStatDedupReplaced,  // inserts that overwrote a live entry of a full window
+    kStatTableAtomics,   // transposition-table atomics issued (claims and depth updates)
+    kStatCommuteSkips,   // children skipped by the partial-order reduction
     kStatCount
 };
 
@@ -107,12 +110,22 @@ constexpr int kInstanceBits = 20;          // up to 1,048,576 instances per laun
 
 // Transposition-table entry.  key = spi packed 5 bits/symbol, 12 per word (n <= 32) or
 // 6 bits/symbol, 10 per word (n <= 63).  tag = generation << 20 | instance.
+// meta = version << 13 | epoch << 5 | best depth.  The version counts the entry's rewrites,
+// so the 64-bit header (tag, meta) read before and after a key read tells whether the key
+// belongs to the header (a seqlock: kernels may overwrite live entries of a full window).
+// The epoch is the write time in units of 2^20 ns (8 bits, so ages up to ~268 ms compare
+// correctly), used by the recency replacement policies.
 template <int KW>
 struct alignas(KW == 3 ? 32 : 64) DedupEntry {
     uint32_t tag;
-    uint32_t depth;
+    uint32_t meta;
     uint64_t key[KW];
 };
+constexpr uint32_t kDepthBits = 5;
+constexpr uint32_t kDepthMask = (1u << kDepthBits) - 1u;
+constexpr uint32_t kEpochShift = 5;
+constexpr uint32_t kEpochMask = 255u << kEpochShift;
+constexpr uint32_t kVersionShift = 13;
 
 struct EngineParams {
     const InstanceIn *in;
@@ -136,6 +149,9 @@ struct EngineParams {
     const uint16_t *order;           // per-instance root child order (learned), or null
     int orderStride;
     int maxInFlight;                 // admitted-but-unfinished instance cap (0 = none)
+    int replace;                     // full-window policy: 0 admit unrecorded, 1 deepest, 2 oldest,
+                                     // 3 deepest then oldest (see dedup_admit)
+    int commute;                     // 1: partial-order reduction of commuting moves (por_skip)
 };
 
 }  // namespace tdp

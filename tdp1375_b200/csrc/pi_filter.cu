@@ -25,6 +25,9 @@
 #include "pi_filter.h"
 
 namespace tdp {
+
+thread_local double gLastFilterKernelMs = 0.0;
+
 namespace {
 
 constexpr int kThreads = 256;
@@ -210,6 +213,167 @@ __global__ void __launch_bounds__(kThreads) pi_filter_write_kernel(const FilterA
     }
 }
 
+// ---------------------------------------------------------------- packed path (n <= 16)
+// With n <= 16 a whole pi fits in one 64-bit register as 4-bit symbols (nibble p = pi[p]),
+// and so does its inverse (nibble s = position of symbol s).  A thread walks kPackedRanks
+// consecutive ranks with next-permutation steps on those two registers (a step rewrites
+// only the suffix it permutes), so no per-thread arrays exist and nothing goes to local
+// memory.  The predicates read positions straight from the inverse:
+//   (1) triple in cyclic order in pi: at most one descent around the triple's positions;
+//   (2) cycle oriented: the cycle is in cyclic order in reversed pi iff its positions have
+//       at most one ascent around the cycle (reversal turns ascents into descents), so the
+//       cycle is kept when it has two or more;
+//   (3) 2-move: the cycle triples (i<j<k in cycle order) whose cycle-distance parities give
+//       after - before == 2 do not depend on pi; the host lists them once (at most
+//       C(16,3) = 560) and a pi has a 2-move iff one listed triple is in cyclic order.
+constexpr int kPackedMaxN = 16;
+constexpr int kPackedRanks = 32;
+constexpr int kPackedRanksPerBlock = kThreads * kPackedRanks;
+constexpr int kMaxTwoMoveTriples = 560;
+
+struct PackedArgs {
+    unsigned long long fact[17];
+    unsigned long long base, total;
+    uint8_t cycle[16];
+    uint8_t triple[16];
+    uint16_t twoMove[kMaxTwoMoveTriples];  // a | b << 4 | c << 8
+    int cycleLen, tripleLen, n, skip2Move, twoMoveCount;
+};
+
+__device__ __forceinline__ uint32_t nib(unsigned long long w, uint32_t i) { return (uint32_t)(w >> (4u * i)) & 15u; }
+__device__ __forceinline__ unsigned long long set_nib(unsigned long long w, uint32_t i, uint32_t v) {
+    return (w & ~(15ull << (4u * i))) | ((unsigned long long)v << (4u * i));
+}
+
+__device__ __forceinline__ void packed_unrank(const PackedArgs &A, unsigned long long r, unsigned long long &pi,
+                                              unsigned long long &inv) {
+    // available symbols 1..n-1 as nibbles, removed one by one (Lehmer digits, highest first)
+    const int n = A.n;
+    unsigned long long avail = 0;
+    for (int i = 0; i < n - 1; ++i) avail |= (unsigned long long)(i + 1) << (4 * i);
+    pi = 0;
+    inv = 0;
+    for (int pos = 1; pos < n; ++pos) {
+        const unsigned long long f = A.fact[n - 1 - pos];
+        const uint32_t choice = (uint32_t)(r / f);
+        r -= (unsigned long long)choice * f;
+        const uint32_t sym = nib(avail, choice);
+        const unsigned long long low = avail & ((1ull << (4 * choice)) - 1ull);
+        const unsigned long long high = (choice + 1 < 16) ? (avail >> (4 * (choice + 1))) << (4 * choice) : 0ull;
+        avail = low | high;
+        pi = set_nib(pi, (uint32_t)pos, sym);
+        inv = set_nib(inv, sym, (uint32_t)pos);
+    }
+}
+
+// Lexicographic successor of pi[1..n-1] (pi[0] = 0 stays), updating the inverse.
+__device__ __forceinline__ void packed_next(int n, unsigned long long &pi, unsigned long long &inv) {
+    int i = n - 2;
+    while (i >= 1 && nib(pi, i) > nib(pi, i + 1)) --i;
+    if (i < 1) return;
+    int j = n - 1;
+    const uint32_t pv = nib(pi, i);
+    while (nib(pi, j) < pv) --j;
+    const uint32_t qv = nib(pi, j);
+    pi = set_nib(set_nib(pi, i, qv), j, pv);
+    for (int l = i + 1, r = n - 1; l < r; ++l, --r) {
+        const uint32_t a = nib(pi, l), b = nib(pi, r);
+        pi = set_nib(set_nib(pi, l, b), r, a);
+    }
+    for (int p = i; p < n; ++p) inv = set_nib(inv, nib(pi, p), (uint32_t)p);
+}
+
+__device__ __forceinline__ bool packed_keep(const PackedArgs &A, unsigned long long inv) {
+    int leaps = 0;
+    for (int t = 0; t < A.tripleLen; ++t) {
+        const uint32_t a = nib(inv, A.triple[t]);
+        const uint32_t b = nib(inv, A.triple[t + 1 == A.tripleLen ? 0 : t + 1]);
+        leaps += a > b ? 1 : 0;
+    }
+    if (leaps > 1) return false;
+    int ascents = 0;
+    for (int t = 0; t < A.cycleLen; ++t) {
+        const uint32_t a = nib(inv, A.cycle[t]);
+        const uint32_t b = nib(inv, A.cycle[t + 1 == A.cycleLen ? 0 : t + 1]);
+        ascents += a < b ? 1 : 0;
+    }
+    if (ascents <= 1) return false;
+    if (A.skip2Move) return true;
+    for (int t = 0; t < A.twoMoveCount; ++t) {
+        const uint32_t w = A.twoMove[t];
+        const uint32_t pa = nib(inv, w & 15u), pb = nib(inv, (w >> 4) & 15u), pc = nib(inv, (w >> 8) & 15u);
+        if ((pa > pb) + (pb > pc) + (pc > pa) <= 1) return false;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(kThreads) packed_count_kernel(const PackedArgs A, unsigned *threadPrefix,
+                                                                 unsigned *blockTotal) {
+    const unsigned long long first =
+        A.base + ((unsigned long long)blockIdx.x * kThreads + threadIdx.x) * kPackedRanks;
+    unsigned hits = 0;
+    if (first < A.total) {
+        unsigned long long pi, inv;
+        packed_unrank(A, first, pi, inv);
+        const unsigned long long last = min(first + kPackedRanks, A.total);
+        for (unsigned long long r = first; r < last; ++r) {
+            hits += packed_keep(A, inv) ? 1u : 0u;
+            packed_next(A.n, pi, inv);
+        }
+    }
+    unsigned total;
+    const unsigned prefix = block_exclusive_scan(hits, &total);
+    threadPrefix[(size_t)blockIdx.x * kThreads + threadIdx.x] = prefix;
+    if (threadIdx.x == 0) blockTotal[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kThreads) packed_write_kernel(const PackedArgs A, const unsigned *threadPrefix,
+                                                                 const unsigned long long *blockOffset, uint8_t *out,
+                                                                 unsigned long long maxRows) {
+    const unsigned long long first =
+        A.base + ((unsigned long long)blockIdx.x * kThreads + threadIdx.x) * kPackedRanks;
+    if (first >= A.total) return;
+    const unsigned next = (threadIdx.x + 1 < kThreads)
+                              ? threadPrefix[(size_t)blockIdx.x * kThreads + threadIdx.x + 1]
+                              : 0xFFFFFFFFu;
+    const unsigned mine = threadPrefix[(size_t)blockIdx.x * kThreads + threadIdx.x];
+    if (next == mine) return;  // no hit among this thread's ranks
+    unsigned long long row = blockOffset[blockIdx.x] + mine;
+    if (row >= maxRows) return;
+    unsigned long long pi, inv;
+    packed_unrank(A, first, pi, inv);
+    const unsigned long long last = min(first + kPackedRanks, A.total);
+    for (unsigned long long r = first; r < last && row < maxRows; ++r) {
+        if (packed_keep(A, inv)) {
+            uint8_t *dst = out + row * (unsigned long long)A.n;
+            for (int i = 0; i < A.n; ++i) dst[i] = (uint8_t)nib(pi, i);
+            ++row;
+        }
+        packed_next(A.n, pi, inv);
+    }
+}
+
+// The host half of the packed path: the pi-independent 2-move triple list
+// (pi_filter.cu:86-115 restated: cycle positions i<j<k, cycle distances a->b, b->c, c->a).
+int two_move_triples(const uint8_t *cycle, int len, uint16_t *out) {
+    uint8_t index[64] = {};
+    for (int i = 0; i < len; ++i) index[cycle[i]] = (uint8_t)i;
+    auto dist = [&](int a, int b) {
+        const int ai = index[a], bi = index[b];
+        return (bi >= ai) ? bi - ai : (len - ai) + bi;
+    };
+    const int before = len & 1;
+    int count = 0;
+    for (int i = 0; i < len - 2; ++i)
+        for (int j = i + 1; j < len - 1; ++j)
+            for (int k = j + 1; k < len; ++k) {
+                const int a = cycle[i], b = cycle[j], c = cycle[k];
+                const int after = (dist(a, b) & 1) + (dist(b, c) & 1) + (dist(c, a) & 1);
+                if (after - before == 2) out[count++] = (uint16_t)(a | (b << 4) | (c << 8));
+            }
+    return count;
+}
+
 // ---------------------------------------------------------------- allocation-free variant
 // Scratch of tdp_pi_filter_noalloc, for callers that cannot allocate device memory: slot 0
 // holds the hit total, slots [1, 1+B) the block offsets and [1+B, 1+2B) the block totals,
@@ -289,10 +453,15 @@ __global__ void __launch_bounds__(kThreads) noalloc_write_kernel(const FilterArg
     }
 }
 
-// Device address of gNoAllocScratch for the current device, looked up once per device
-// (with that device current) and cached.
+// Device address of gNoAllocScratch for the current device.  It is looked up
+// (cudaGetSymbolAddress, with that device current) on the first call on a device and cached
+// together with the device's current context, and looked up again when that context has
+// changed (after cudaDeviceReset the old address is stale).
 unsigned long long *noalloc_scratch(std::string &err) {
+    using CtxGetCurrent = int (*)(void **);
     static std::mutex mu;
+    static CtxGetCurrent ctxGetCurrent = nullptr;
+    static void *ctxOf[64] = {};
     static unsigned long long *addr[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
@@ -300,13 +469,28 @@ unsigned long long *noalloc_scratch(std::string &err) {
         return nullptr;
     }
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
+    if (!ctxGetCurrent) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            err = "tdp_pi_filter_noalloc: cuCtxGetCurrent is not available";
+            return nullptr;
+        }
+        ctxGetCurrent = reinterpret_cast<CtxGetCurrent>(fn);
+    }
+    void *ctx = nullptr;
+    if (!addr[dev] || ctxGetCurrent(&ctx) != 0 || ctx != ctxOf[dev]) {
         void *ptr = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&ptr, gNoAllocScratch);
         if (e != cudaSuccess || !ptr) {
             err = std::string("tdp_pi_filter_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
             return nullptr;
         }
+        // the runtime has made the device's primary context current by now
+        ctx = nullptr;
+        if (ctxGetCurrent(&ctx) != 0) ctx = nullptr;
+        ctxOf[dev] = ctx;
         addr[dev] = static_cast<unsigned long long *>(ptr);
     }
     return addr[dev];
@@ -368,8 +552,24 @@ int64_t pi_filter_run(const uint8_t *cycle, int cycleLen, const uint8_t *triple,
     A.skip2Move = skip2Move ? 1 : 0;
     A.total = A.fact[n - 1 > 0 ? n - 1 : 0];
 
+    // n <= 16 (with cycle and triple of at most 16 symbols) takes the packed-register kernels
+    const bool packed = n <= kPackedMaxN && cycleLen <= 16 && tripleLen <= 16;
+    PackedArgs P;
+    std::memset(&P, 0, sizeof(P));
+    if (packed) {
+        for (int i = 0; i <= 16; ++i) P.fact[i] = A.fact[i];
+        P.total = A.total;
+        std::memcpy(P.cycle, cycle, cycleLen);
+        std::memcpy(P.triple, triple, tripleLen);
+        P.cycleLen = cycleLen;
+        P.tripleLen = tripleLen;
+        P.n = n;
+        P.skip2Move = A.skip2Move;
+        P.twoMoveCount = two_move_triples(cycle, cycleLen, P.twoMove);
+    }
+    const int ranksPerBlock = packed ? kPackedRanksPerBlock : kRanksPerBlock;
     const uint64_t launchRanks = std::min<uint64_t>(kLaunchRanks, A.total);
-    const int maxBlocks = (int)((launchRanks + kRanksPerBlock - 1) / kRanksPerBlock);
+    const int maxBlocks = (int)((launchRanks + ranksPerBlock - 1) / ranksPerBlock);
     DeviceBuffer prefix, totals, offsets, grand, rows;
     if (!ok(cudaMalloc(&prefix.ptr, (size_t)maxBlocks * kThreads * sizeof(unsigned)), err, "cudaMalloc") ||
         !ok(cudaMalloc(&totals.ptr, (size_t)maxBlocks * sizeof(unsigned)), err, "cudaMalloc") ||
@@ -380,26 +580,56 @@ int64_t pi_filter_run(const uint8_t *cycle, int cycleLen, const uint8_t *triple,
     const size_t outBytes = (size_t)std::max<int64_t>(maxRows, 1) * (size_t)n;
     if (maxRows > 0 && !ok(cudaMalloc(&rows.ptr, outBytes), err, "cudaMalloc(rows)")) return -4;
 
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!ok(cudaEventCreate(&e0), err, "cudaEventCreate") || !ok(cudaEventCreate(&e1), err, "cudaEventCreate")) {
+        if (e0) cudaEventDestroy(e0);
+        return -3;
+    }
+    float kernelMs = 0.f;
     const auto start = std::chrono::steady_clock::now();
-    for (uint64_t base = 0; base < A.total; base += kLaunchRanks) {
+    int64_t rc = 0;
+    for (uint64_t base = 0; base < A.total && rc == 0; base += kLaunchRanks) {
         A.base = base;
+        P.base = base;
         const uint64_t ranks = std::min<uint64_t>(kLaunchRanks, A.total - base);
-        const int blocks = (int)((ranks + kRanksPerBlock - 1) / kRanksPerBlock);
-        pi_filter_count_kernel<<<blocks, kThreads>>>(A, (unsigned *)prefix.ptr, (unsigned *)totals.ptr);
+        const int blocks = (int)((ranks + ranksPerBlock - 1) / ranksPerBlock);
+        cudaEventRecord(e0);
+        if (packed) {
+            packed_count_kernel<<<blocks, kThreads>>>(P, (unsigned *)prefix.ptr, (unsigned *)totals.ptr);
+        } else {
+            pi_filter_count_kernel<<<blocks, kThreads>>>(A, (unsigned *)prefix.ptr, (unsigned *)totals.ptr);
+        }
         pi_filter_scan_kernel<<<1, kThreads>>>((const unsigned *)totals.ptr, (unsigned long long *)offsets.ptr,
                                                blocks, (unsigned long long *)grand.ptr);
-        if (maxRows > 0)
-            pi_filter_write_kernel<<<blocks, kThreads>>>(A, (const unsigned *)prefix.ptr,
-                                                         (const unsigned long long *)offsets.ptr,
-                                                         (uint8_t *)rows.ptr, (unsigned long long)maxRows);
-        if (!ok(cudaGetLastError(), err, "pi filter launch")) return -3;
-        if (!ok(cudaDeviceSynchronize(), err, "pi filter")) return -3;
+        if (maxRows > 0) {
+            if (packed) {
+                packed_write_kernel<<<blocks, kThreads>>>(P, (const unsigned *)prefix.ptr,
+                                                          (const unsigned long long *)offsets.ptr,
+                                                          (uint8_t *)rows.ptr, (unsigned long long)maxRows);
+            } else {
+                pi_filter_write_kernel<<<blocks, kThreads>>>(A, (const unsigned *)prefix.ptr,
+                                                             (const unsigned long long *)offsets.ptr,
+                                                             (uint8_t *)rows.ptr, (unsigned long long)maxRows);
+            }
+        }
+        cudaEventRecord(e1);
+        if (!ok(cudaGetLastError(), err, "pi filter launch") || !ok(cudaDeviceSynchronize(), err, "pi filter")) {
+            rc = -3;
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        kernelMs += ms;
         const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
         if (base + kLaunchRanks < A.total && elapsed > timeLimitS) {
             err = "pi filter: time limit exceeded";
-            return -5;
+            rc = -5;
         }
     }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != 0) return rc;
+    gLastFilterKernelMs = kernelMs;
     unsigned long long hits = 0;
     if (!ok(cudaMemcpy(&hits, grand.ptr, sizeof(hits), cudaMemcpyDeviceToHost), err, "read count")) return -3;
     const int64_t kept = std::min<int64_t>((int64_t)hits, maxRows);
@@ -448,8 +678,9 @@ int64_t pi_filter_noalloc_run(const uint8_t *cycle, int cycleLen, const uint8_t 
     A.total = A.fact[n - 1 > 0 ? n - 1 : 0];
     A.base = 0;
     const int blocks = (int)((A.total + kRanksPerBlock - 1) / kRanksPerBlock);
-    // The scratch keeps the previous call's contents: the hit total starts at zero.
-    if (!ok(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), stream), err, "tdp_pi_filter_noalloc")) return -3;
+    // The scratch keeps the previous call's contents; nothing needs clearing: the count pass
+    // writes every block total the scan reads, and the scan writes every offset the write
+    // pass reads and the hit total.
     noalloc_count_kernel<<<blocks, kThreads, 0, stream>>>(A, scratch, blocks);
     noalloc_scan_kernel<<<1, kThreads, 0, stream>>>(scratch, blocks);
     if (maxRows > 0)

@@ -13,6 +13,9 @@ namespace tdp {
 int64_t pi_filter_run(const uint8_t *cycle, int cycleLen, const uint8_t *triple, int tripleLen, int n,
                       int skip2Move, uint8_t *out, int64_t maxRows, double timeLimitS, std::string &err);
 
+// Device time (CUDA events around the kernels) of the calling thread's last pi_filter_run.
+extern thread_local double gLastFilterKernelMs;
+
 // Allocation-free variant (n <= 12): scratch is a static device array, rows go to a
 // caller-provided device buffer, work runs on `stream`.  Same return convention.
 int64_t pi_filter_noalloc_run(const uint8_t *cycle, int cycleLen, const uint8_t *triple, int tripleLen, int n,

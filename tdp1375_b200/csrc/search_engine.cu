@@ -309,6 +309,8 @@ void SearchSlot::launchClass(int cls, int offset, int count) {
     P.sparse = cfg_.sparse_enumeration;
     P.order = (cls == 0 && orderedLaunch_) ? dOrder_ : nullptr;
     P.orderStride = combinations3(32);
+    P.replace = cfg_.table_replacement;
+    P.commute = cfg_.commute;
 
     int blocksPerSM = 0;
     const int threads = dev::kWarpsPerBlock * 32;
@@ -568,6 +570,9 @@ tdp_stats SearchSlot::stats() const {
     s.task_pops = statsAccum_[kStatTaskPops];
     s.busy_warp_cycles = statsAccum_[kStatBusyCycles];
     s.warp_cycles = statsAccum_[kStatWarpCycles];
+    s.dedup_replaced = statsAccum_[kStatDedupReplaced];
+    s.table_atomics = statsAccum_[kStatTableAtomics];
+    s.commute_skips = statsAccum_[kStatCommuteSkips];
     s.kernel_ms = kernelMs_;
     s.error = deviceError_;
     s.launches = launches_;

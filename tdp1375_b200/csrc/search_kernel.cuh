@@ -196,81 +196,190 @@ __device__ __forceinline__ uint64_t key_hash(const uint64_t (&k)[KW], uint32_t t
     return h;
 }
 
-// Outcome bits of dedup_admit: admitted, inserted into an empty or reclaimed entry, or
-// admitted without an entry because the window was full.
-constexpr uint32_t kAdmitted = 1u, kInserted = 2u, kWindowFull = 4u;
+// Outcome bits of dedup_admit: admitted, inserted into an empty, reclaimed or replaced
+// entry, admitted without an entry because the window was full, inserted over a live entry
+// of a full window, and "issued an atomic" (a claim or a depth update, for the statistics).
+constexpr uint32_t kAdmitted = 1u, kInserted = 2u, kWindowFull = 4u, kReplaced = 8u, kAtomic = 16u;
 
-// Transposition-table admission (sorting_search.cu:261-298 semantics, per instance).
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const void *p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(void *p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t cas_acq_rel_u64(void *p, uint64_t cmp, uint64_t val) {
+    uint64_t old;
+    asm volatile("atom.acq_rel.gpu.global.cas.b64 %0, [%1], %2, %3;"
+                 : "=l"(old)
+                 : "l"(p), "l"(cmp), "l"(val)
+                 : "memory");
+    return old;
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Transposition-table admission (sorting_search.cu:261-298 semantics, per instance): a
+// state of the same instance admitted at a depth <= `depth` prunes it; otherwise it is
+// admitted and recorded.
+//
+// Entries are written under a claim: a 64-bit CAS of the header (tag, meta) from the value
+// read to (kTagWriting, version + 1 | epoch | depth) with acquire-release order, then the
+// key, then a release store of the tag.  With P.replace = 0 only empty entries and entries
+// of older generations or finished instances are claimed, so an entry that carries this
+// instance's tag is never rewritten while the instance runs: a key read after the tag is
+// that entry's key, and best depths only decrease.  With P.replace > 0 a full window also
+// claims one of its live entries (policy 1: the deepest, if at least as deep as the
+// newcomer; 2: the oldest; 3: the deepest, the oldest among those), so a key read may race
+// with a rewrite.  A prune then counts only if the header read again after the key (behind
+// a fence) is unchanged: the rewrite's claim changes the header before any key store, and
+// the version never repeats.  A depth improvement is a CAS of the header read, which also
+// fails after a rewrite.  A failed check admits the child, which only costs work.
 template <int KW>
 __device__ __forceinline__ uint32_t dedup_admit(const EngineParams &P, uint32_t generation, uint32_t tag,
                                             const uint64_t (&key)[KW], uint64_t h, uint32_t depth) {
     auto *table = reinterpret_cast<DedupEntry<KW> *>(P.table);
     const uint32_t base = (uint32_t)(h >> 24) & P.tableMask & ~7u;
-    // Eight independent relaxed tag loads (one round trip); only when a tag matches does the
-    // lane pay an acquire fence before reading keys, which pairs with the release store that
-    // published the entry.  (Eight acquire loads would serialise into eight round trips.)
-    uint32_t tags[8];
+    const uint32_t epoch = (uint32_t)(global_time_ns() >> 20) & 255u;
+    // Eight independent relaxed header loads (one round trip); only when a tag matches does
+    // the lane pay an acquire fence before reading keys, which pairs with the release store
+    // that published the entry.
+    uint64_t hdr[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) tags[q] = ld_relaxed_u32(&table[base + q].tag);
-    bool anyMatch = false;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) anyMatch |= (tags[q] == tag);
-    if (anyMatch) asm volatile("fence.acq_rel.gpu;" ::: "memory");
-    unsigned freeMask = 0;
+    for (int q = 0; q < 8; ++q) hdr[q] = ld_relaxed_u64(&table[base + q]);
+    unsigned tagMask = 0, freeMask = 0, liveMask = 0;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const uint32_t t = tags[q];
+        const uint32_t t = (uint32_t)hdr[q];
         if (t == tag) {
-            DedupEntry<KW> *e = &table[base + q];
-            bool eq = true;
-#pragma unroll
-            for (int kq = 0; kq < KW; ++kq) eq &= (__ldcg(&e->key[kq]) == key[kq]);
-            // Best depths only decrease, so a value read after the fence that is already
-            // <= depth decides the prune without an atomic.
-            const uint32_t seen = ld_relaxed_u32(&e->depth);
-            if (eq && seen <= depth) return 0u;
-            if (eq) {
-                const uint32_t prev = atomicMin(&e->depth, depth);
-                return prev <= depth ? 0u : kAdmitted;
-            }
+            tagMask |= 1u << q;
         } else if (t == 0u || (t != kTagWriting && (t >> kInstanceBits) != generation)) {
             freeMask |= 1u << q;
+        } else if (t != kTagWriting) {
+            liveMask |= 1u << q;
         }
     }
+    if (tagMask) {
+        fence_acq_rel_gpu();
+        // the keys of every entry with this instance's tag, loaded together
+        unsigned eqMask = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if ((tagMask >> q) & 1u) {
+                const DedupEntry<KW> *e = &table[base + q];
+                bool eq = true;
+#pragma unroll
+                for (int kq = 0; kq < KW; ++kq) eq &= (ld_relaxed_u64(&e->key[kq]) == key[kq]);
+                eqMask |= (eq ? 1u : 0u) << q;
+            }
+        }
+        if (eqMask) {
+            const int m = __ffs(eqMask) - 1;
+            uint64_t hm = 0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (q == m) hm = hdr[q];
+            DedupEntry<KW> *e = &table[base + m];
+            const uint32_t mm = (uint32_t)(hm >> 32);
+            if (P.replace) {
+                if ((mm & kDepthMask) <= depth) {
+                    fence_acq_rel_gpu();
+                    return ld_relaxed_u64(e) == hm ? 0u : kAdmitted;
+                }
+                const uint32_t nm = (mm & ~(kDepthMask | kEpochMask)) | (epoch << kEpochShift) | depth;
+                cas_acq_rel_u64(e, hm, ((uint64_t)nm << 32) | tag);
+                return kAdmitted | kAtomic;
+            }
+            // Best depths only decrease, so a header value that is already <= depth decides
+            // the prune without an atomic.
+            if ((mm & kDepthMask) <= depth) return 0u;
+            const uint32_t prev = atomicMin(&e->meta, (mm & ~kDepthMask) | depth);
+            return (prev & kDepthMask) <= depth ? kAtomic : (kAdmitted | kAtomic);
+        }
+        liveMask |= tagMask;
+    }
     if (freeMask == 0u) {
-        // No empty or old-generation slot: look for entries of finished instances, with
-        // the eight done-bit loads issued together.
+        // No empty or old-generation entry: entries of finished instances are free too
+        // (their done bits, loaded together).
         uint32_t done[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            const uint32_t idx = tags[q] & ((1u << kInstanceBits) - 1u);
-            done[q] = (tags[q] != kTagWriting) ? ld_relaxed_u32(P.doneBits + (idx >> 5)) : 0u;
+            const uint32_t idx = (uint32_t)hdr[q] & ((1u << kInstanceBits) - 1u);
+            done[q] = ((liveMask >> q) & 1u) ? ld_relaxed_u32(P.doneBits + (idx >> 5)) : 0u;
         }
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            const uint32_t idx = tags[q] & ((1u << kInstanceBits) - 1u);
-            if (tags[q] != kTagWriting && ((done[q] >> (idx & 31u)) & 1u)) freeMask |= 1u << q;
+            const uint32_t idx = (uint32_t)hdr[q] & ((1u << kInstanceBits) - 1u);
+            if ((done[q] >> (idx & 31u)) & 1u) freeMask |= 1u << q;
         }
     }
-    const int freeSlot = freeMask ? (__ffs(freeMask) - 1) : -1;
-    // an unrolled select keeps the tags in registers (a dynamic index would put them in
+    int slot = freeMask ? (__ffs(freeMask) - 1) : -1;
+    uint32_t outcome = kAdmitted | kInserted;
+    if (slot < 0) {
+        if (!P.replace) return kAdmitted | kWindowFull;
+        // The victim: policy 1 the deepest live entry at least as deep as the newcomer
+        // (shallow entries prune the largest subtrees); 2 the oldest live entry; 3 the
+        // deepest, the oldest among equally deep ones.  Ties go to the later slot.
+        uint32_t best = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t m = (uint32_t)(hdr[q] >> 32);
+            const uint32_t d = m & kDepthMask;
+            const uint32_t age = (epoch - ((m & kEpochMask) >> kEpochShift)) & 255u;
+            const uint32_t score = P.replace == 1 ? (d >= depth ? d + 1u : 0u)
+                                   : P.replace == 2 ? age + 1u
+                                                    : ((d << 8) | age) + 1u;
+            if (((liveMask >> q) & 1u) && score >= best && score > 0u) {
+                best = score;
+                slot = q;
+            }
+        }
+        if (slot < 0) return kAdmitted | kWindowFull;
+        outcome |= kReplaced;
+    }
+    // an unrolled select keeps the headers in registers (a dynamic index would put them in
     // local memory on every probe)
-    uint32_t freeTag = 0u;
+    uint64_t old = 0;
 #pragma unroll
     for (int q = 0; q < 8; ++q)
-        if (q == freeSlot) freeTag = tags[q];
-    if (freeSlot >= 0) {
-        DedupEntry<KW> *e = &table[base + freeSlot];
-        if (atomicCAS(&e->tag, freeTag, kTagWriting) == freeTag) {
-            e->depth = depth;
+        if (q == slot) old = hdr[q];
+    DedupEntry<KW> *e = &table[base + slot];
+    const uint32_t version = ((uint32_t)(old >> 32) >> kVersionShift) + 1u;
+    const uint64_t claim =
+        ((uint64_t)((version << kVersionShift) | (epoch << kEpochShift) | depth) << 32) | kTagWriting;
+    if (cas_acq_rel_u64(e, old, claim) != old) return kAdmitted | kAtomic;
 #pragma unroll
-            for (int kq = 0; kq < KW; ++kq) __stcg(&e->key[kq], key[kq]);
-            st_release_u32(&e->tag, tag);  // the release orders the depth and key stores before it
-            return kAdmitted | kInserted;
-        }
-        return kAdmitted;
-    }
-    return kAdmitted | kWindowFull;
+    for (int kq = 0; kq < KW; ++kq) st_relaxed_u64(&e->key[kq], key[kq]);
+    st_release_u32(&e->tag, tag);  // the release orders the key stores before it
+    return outcome | kAtomic;
+}
+
+// Partial-order reduction of commuting moves (verdict-preserving; no counterpart in the
+// reference).  The node of frame f was reached by the move (x y z) at positions I<J<K of its
+// parent P; its child (a b c) at positions i<j<k is skipped when {a,b,c} and {x,y,z} are
+// disjoint, (a b c) is also a move at P (a, b, c in cyclic order there: the inverse block
+// swap of (I,J,K) gives their positions in P), (x y z) is a move once (a b c) has been
+// applied at P, and min(a,b,c) < min(x,y,z).  Disjoint 3-cycles commute, so P.(a b c).(x y z)
+// reaches the same state at the same depth through the kept order.  Every admission
+// condition of the rule tables is monotone along a move sequence (a move changes the
+// odd-cycle count by at most 2), so the kept order passes them wherever the skipped one
+// does; a state's subtree is explored from its first admission, and any child that
+// admission skips is reached through its parent's commuted sibling, by induction on depth
+// and then on the move order.
+__device__ __forceinline__ bool por_skip(uint32_t inc, uint32_t x, uint32_t y, uint32_t z, uint32_t i, uint32_t j,
+                                         uint32_t k, uint32_t a, uint32_t b, uint32_t c) {
+    if (a == x || a == y || a == z || b == x || b == y || b == z || c == x || c == y || c == z) return false;
+    const int I = (int)tri_i(inc), J = (int)tri_j(inc), K = (int)tri_k(inc);
+    const int pa = block_swap_src((int)i, I, J, K), pb = block_swap_src((int)j, I, J, K),
+              pc = block_swap_src((int)k, I, J, K);
+    if ((pa > pb) + (pb > pc) + (pc > pa) > 1) return false;
+    const int q0 = min(pa, min(pb, pc)), q2 = max(pa, max(pb, pc)), q1 = pa + pb + pc - q0 - q2;
+    const int lenA = q1 - q0, lenB = q2 - q1;
+    const int fI = (I >= q0 && I < q1) ? I + lenB : (I >= q1 && I < q2) ? I - lenA : I;
+    const int fJ = (J >= q0 && J < q1) ? J + lenB : (J >= q1 && J < q2) ? J - lenA : J;
+    const int fK = (K >= q0 && K < q1) ? K + lenB : (K >= q1 && K < q2) ? K - lenA : K;
+    if ((fI > fJ) + (fJ > fK) + (fK > fI) > 1) return false;
+    return min(a, min(b, c)) < min(x, min(y, z));
 }
 
 // Idle-warp ring: a bounded lock-free multi-producer/multi-consumer queue of warp ids.  Slot
@@ -923,7 +1032,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                     outcome = 1;
                     break;
                 }
-                const bool probe = valid && ((expMask >> e) & 1ull);
+                bool probe = valid && ((expMask >> e) & 1ull);
+                if (P.commute && f > 0) {
+                    // the move that reached this frame and its symbols (y now at I, x at I+K-J, z at K)
+                    const uint32_t inc = S.frames[f - 1].move;
+                    const uint32_t I = tri_i(inc), J = tri_j(inc), K = tri_k(inc);
+                    const uint32_t y = w_pi(gather<NW>(w, I)), x = w_pi(gather<NW>(w, I + K - J)),
+                                   z = w_pi(gather<NW>(w, K));
+                    const bool skip = probe && por_skip(inc, x, y, z, tri_i(tr), tri_j(tr), tri_k(tr), a, b, c);
+                    const unsigned skipped = __ballot_sync(kFull, skip);
+                    if (lane == 0) S.stats[kStatCommuteSkips] += (unsigned)__popc(skipped);
+                    probe = probe && !skip;
+                }
                 const unsigned probing = __ballot_sync(kFull, probe);
                 uint32_t outc = 0u;
                 if (probe) {
@@ -936,14 +1056,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                     outc = dedup_admit<KW>(P, generation, tag, ck, key_hash<KW>(ck, tag), (uint32_t)(f + 1));
                 }
                 pending = __ballot_sync(kFull, outc & kAdmitted);
+                const unsigned atomics = __ballot_sync(kFull, outc & kAtomic);
                 if (probing) {
                     const unsigned ins = __ballot_sync(kFull, outc & kInserted);
                     const unsigned full = __ballot_sync(kFull, outc & kWindowFull);
+                    const unsigned repl = __ballot_sync(kFull, outc & kReplaced);
                     if (lane == 0) {
                         S.stats[kStatDedupProbes] += (unsigned)__popc(probing);
                         S.stats[kStatDedupPruned] += (unsigned)__popc(probing & ~pending);
                         S.stats[kStatDedupInserts] += (unsigned)__popc(ins);
                         S.stats[kStatDedupFull] += (unsigned)__popc(full);
+                        S.stats[kStatDedupReplaced] += (unsigned)__popc(repl);
+                        S.stats[kStatTableAtomics] += (unsigned)__popc(atomics);
                     }
                 }
                 continue;
@@ -1046,6 +1170,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
         atomicAdd(&ctl->stats[kStatDedupFull], S.stats[kStatDedupFull]);
         atomicAdd(&ctl->stats[kStatDonations], S.stats[kStatDonations]);
         atomicAdd(&ctl->stats[kStatTaskPops], S.stats[kStatTaskPops]);
+        atomicAdd(&ctl->stats[kStatDedupReplaced], S.stats[kStatDedupReplaced]);
+        atomicAdd(&ctl->stats[kStatTableAtomics], S.stats[kStatTableAtomics]);
+        atomicAdd(&ctl->stats[kStatCommuteSkips], S.stats[kStatCommuteSkips]);
         S.stats[kStatWarpCycles] += (unsigned long long)clock64();
         atomicAdd(&ctl->stats[kStatBusyCycles], S.stats[kStatBusyCycles]);
         atomicAdd(&ctl->stats[kStatWarpCycles], S.stats[kStatWarpCycles]);

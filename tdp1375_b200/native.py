@@ -31,14 +31,17 @@ class Stats(ctypes.Structure):
                 ("dedup_pruned", ctypes.c_uint64), ("dedup_inserts", ctypes.c_uint64), ("dedup_full", ctypes.c_uint64),
                 ("donations", ctypes.c_uint64), ("task_pops", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
                 ("error", ctypes.c_int32), ("launches", ctypes.c_int32),
-                ("busy_warp_cycles", ctypes.c_uint64), ("warp_cycles", ctypes.c_uint64)]
+                ("busy_warp_cycles", ctypes.c_uint64), ("warp_cycles", ctypes.c_uint64),
+                ("dedup_replaced", ctypes.c_uint64), ("table_atomics", ctypes.c_uint64),
+                ("commute_skips", ctypes.c_uint64)]
 
 
 class EngineConfig(ctypes.Structure):
     _fields_ = [("blocks_per_sm", ctypes.c_int32), ("poll_interval", ctypes.c_int32), ("tight_bound", ctypes.c_int32),
                 ("task_capacity", ctypes.c_int32), ("time_limit_s", ctypes.c_double),
                 ("sparse_enumeration", ctypes.c_int32), ("use_cuda_graph", ctypes.c_int32),
-                ("warps_per_instance", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("warps_per_instance", ctypes.c_int32), ("table_replacement", ctypes.c_int32),
+                ("commute", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 assert ctypes.sizeof(Instance) == 136 and ctypes.sizeof(Result) == 208
@@ -58,6 +61,7 @@ SIGNATURES = {
     "tdp_cancel": (ctypes.c_int, [ctypes.c_int]),
     "tdp_pi_filter": (ctypes.c_int64, [u8p, ctypes.c_int, u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int, u8p,
                                        ctypes.c_int64]),
+    "tdp_pi_filter_last_kernel_ms": (ctypes.c_double, []),
     "tdp_search_batch": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Instance), ctypes.c_int, ctypes.c_float,
                                         ctypes.POINTER(Result)]),
     "tdp_batch_prepare": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Instance), ctypes.c_int, ctypes.c_float]),
@@ -85,6 +89,9 @@ SIGNATURES = {
     "tdp_extension_count": (ctypes.c_int, [ctypes.c_int]),
     "tdp_extension_filter": (ctypes.c_int64, [vp, vp, ctypes.c_int, ctypes.c_int, vp]),
     "tdp_extension_filter_device": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]),
+    "tdp_measure_atomics": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_double)]),
+    "tdp_measure_last_error": (ctypes.c_char_p, []),
     "tdp_pi_filter_noalloc": (ctypes.c_int64, [u8p, ctypes.c_int, u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
                                                ctypes.c_int64, vp]),
 }

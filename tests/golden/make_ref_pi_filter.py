@@ -4,7 +4,9 @@ performGpuPiFilter (pi_filter.cu:157-260, compiled from the reference sources by
 `make -C oracle ref` and driven by oracle/ref_harness.cu) runs on a B200 over seeded
 (cycle, oriented triple) inputs for n = 4..11, with and without the 2-move check.  The
 reference appends rows in an arbitrary order, so each record keeps the number of rows and
-the SHA-256 of the rows sorted as byte strings (and the rows themselves for n <= 7):
+the SHA-256 of the rows sorted as byte strings (and the rows themselves for n <= 7), for the
+optimised build and, when it is built (make -C oracle ref-debug), for the build whose
+device code is unoptimised:
 
     python tests/golden/make_ref_pi_filter.py [--out PATH]
 """
@@ -23,7 +25,10 @@ sys.path.insert(0, ROOT)
 
 
 def inputs():
-    """The seeded filter inputs: (n, cycle, oriented triple) with the triple inside the cycle."""
+    """The filter inputs: (n, cycle, oriented triple) with the triple's symbols in the cycle.
+    Seeded draws for n = 4..11, plus inputs whose triple runs against the cycle's own order
+    (the three symbols in reverse cyclic order), where the triple condition and the
+    orientation condition can exclude each other."""
     rng = np.random.Generator(np.random.PCG64(1375 + 3 * 10**6 + 777))
     out = []
     for n in range(4, 12):
@@ -32,6 +37,8 @@ def inputs():
             cycle = [int(v) for v in rng.permutation(n)[:length]]
             triple = [int(v) for v in rng.choice(cycle, 3, replace=False)]
             out.append((n, cycle, triple))
+    out += [(4, [1, 2, 3], [3, 2, 1]), (6, [4, 2, 5, 1], [5, 2, 4]), (7, [1, 3, 4, 2], [1, 2, 3]),
+            (9, [8, 3, 5], [3, 8, 5]), (10, [1, 9, 4], [1, 4, 9]), (10, [9, 1, 3, 5, 7, 2, 0], [1, 0, 5])]
     return out
 
 
@@ -48,6 +55,7 @@ def main():
     args = p.parse_args()
     from oracle import reference_gpu as R
     records = []
+    debug = R.available(debug=True)
     for n, cycle, triple in inputs():
         for skip in (False, True):
             rows = R.pi_filter(cycle, triple, n, skip)
@@ -55,11 +63,18 @@ def main():
                    "sha256_sorted": digest(rows)}
             if n <= 7:
                 rec["sorted_rows"] = [list(r) for r in rows]
+            if debug:
+                rows_g = R.pi_filter(cycle, triple, n, skip, debug=True)
+                rec["unoptimised"] = {"rows": len(rows_g), "sha256_sorted": digest(rows_g)}
+                if n <= 7:
+                    rec["unoptimised"]["sorted_rows"] = [list(r) for r in rows_g]
             records.append(rec)
+    differs = sum(1 for r in records if "unoptimised" in r and r["unoptimised"]["rows"] < (1 << 20) and
+                  r["unoptimised"]["sha256_sorted"] != r["sha256_sorted"])
     with open(args.out, "w") as fh:
         json.dump({"source": "reference pi_filter.cu:157-260 (performGpuPiFilter) on one B200, built by "
-                             "oracle/Makefile (ref) and driven by oracle/ref_harness.cu",
-                   "records": records}, fh, separators=(",", ":"))
+                             "oracle/Makefile (targets ref and ref-debug) and driven by oracle/ref_harness.cu",
+                   "optimised_build_differs": differs, "records": records}, fh, separators=(",", ":"))
     print(len(records), "records")
 
 

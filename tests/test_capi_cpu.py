@@ -27,8 +27,8 @@ def test_struct_layouts():
     from tdp1375_b200 import native
     assert ctypes.sizeof(native.Instance) == 136
     assert ctypes.sizeof(native.Result) == 208
-    assert ctypes.sizeof(native.Stats) == 8 * 8 + 8 + 8 + 2 * 8
-    assert ctypes.sizeof(native.EngineConfig) == 40
+    assert ctypes.sizeof(native.Stats) == 8 * 8 + 8 + 8 + 5 * 8
+    assert ctypes.sizeof(native.EngineConfig) == 48
 
 
 def test_errors_without_slots(native_lib):

@@ -1,4 +1,5 @@
-"""GPU parity of the permutation filter against the CPU restatement of pi_filter.cu."""
+"""GPU parity of the permutation filter against the CPU restatement of pi_filter.cu, in rank
+order, n = 1..11 (the packed-register kernels serve every n <= 16)."""
 import numpy as np
 import pytest
 
@@ -7,8 +8,8 @@ pytestmark = pytest.mark.gpu
 
 def cases():
     rng = np.random.Generator(np.random.PCG64(1375))
-    out = []
-    for n in (5, 7, 8, 9, 10):
+    out = [(1, [0], [0]), (2, [0, 1], [1, 0]), (3, [0, 1, 2], [0, 1, 2]), (3, [2, 1, 0], [0, 1, 2])]
+    for n in (4, 5, 7, 8, 9, 10, 11):
         for _ in range(3):
             cl = int(rng.integers(3, n + 1))
             cycle = [int(v) for v in rng.permutation(n)[:cl]]
@@ -23,7 +24,8 @@ def test_pi_filter_matches_oracle(native_lib, oracle, skip):
     for n, cycle, triple in cases():
         hits, rows = oracle.pi_filter(cycle, triple, n, skip)
         got = GPUSortingSearch.filterPiPermutations(cycle, len(cycle), triple, len(triple), n, skip)
-        assert len(got) == hits and got == rows, (n, cycle, triple)
+        # at most 1,048,576 rows come back (MAX_OUTPUT, pi_filter.cu:16), the first ones in rank order
+        assert len(got) == min(hits, 1 << 20) and got == rows, (n, cycle, triple)
 
 
 def test_pi_filter_row_limit_and_count(native_lib, oracle):
