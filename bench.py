@@ -1,18 +1,32 @@
 """Benchmark: cases resolved/s (and nodes/s) of the transposition-sequence search on B200.
 
-Workload: 3-permutation configurations of the tdp1375 proof (spi = product of m disjoint
-3-cycles on n = 3m symbols, pi = identity), m ~ U{4..8}, seeded case by case
-(seed 1375 + 2*10**6 + case) over a 100,000-case set; full sorting, ratio 1.375
-(minRate = float32(2)/float32(1.375)), max depth 11, queue budget 3000 MB, one slot.  The
-transposition table holds 2^30 entries (32 GB): a full-sorting m=8 instance inserts ~36M
-states, and a saturated table multiplies the explored nodes (2^27 entries: 15x more nodes).  A step is one batch of --batch consecutive cases
-(step s of rank r covers cases [(s*N + r)*B, (s*N + r + 1)*B) mod 100,000).
+Headline workload: 3-permutation configurations of the tdp1375 proof
+(spi = product of m disjoint 3-cycles on n = 3m symbols, pi = identity), m ~ U{4..8},
+seeded case by case (seed 1375 + 2*10**6 + case) over a 100,000-case set; full sorting,
+ratio 1.375 (minRate = float32(2)/float32(1.375)), max depth 11, queue budget 3000 MB, one
+slot, a transposition table of 2,097,152 entries (2M, as the reference's dedupTableSize).  A
+step is one batch of --batch consecutive cases (step s of rank r covers cases
+[(s*N + r)*B, (s*N + r + 1)*B) mod 100,000).
 
 value: cases/s with the step's instances already resident in HBM (tdp_batch_prepare before
 the timed region; tdp_batch_run timed with CUDA events on the engine's stream), L2 flushed
 with a 256 MB write between steps.  e2e: the same steps through tdp_search_batch with host
-buffers (upload, run, download inside the timed region).  --impl reference times the CPU
-restatement of the reference's CPU search (SortingSearch.java) on the host cores.
+buffers (upload, run, download inside the timed region).
+
+Extra objects on the same line, each a bounded measurement:
+  table_2p30     the headline steps on a 2^30-entry table (32 GB);
+  learned        plain vs learned root order on held-out m = 8..10 configurations (partial
+                 mode, depth 11, the model trained in the untimed warm-up) and on full-sorting
+                 m = 6..7 configurations with exhaustive negatives;
+  dropin         SortOrExtend's call pattern: tdp_search one configuration per call, staged
+                 depths 4 -> 8 -> 11 in partial mode, over the reference's cases-comb.txt;
+  reference_gpu  the reference's own CUDA search (built from its sources into oracle/_ref) on
+                 the first headline step's cases and on the drop-in calls, per-case limits;
+  atomics        the engine's table atomics per second against a measured L2 atomic roof;
+  pi_filter      the permutation filter (tdp_pi_filter) at n = 11 and 12 beside the
+                 reference's performGpuPiFilter on the same inputs.
+--impl reference times the CPU restatement of the reference's CPU search (SortingSearch.java)
+on the host cores.
 """
 from __future__ import annotations
 
@@ -30,13 +44,10 @@ sys.path.insert(0, ROOT)
 TOTAL_CASES = 100_000
 CONFIG = 2
 MAX_DEPTH = 11
-DEDUP_ENTRIES = 1 << 30  # 32 GB of 32-byte entries: room for every concurrent m=8 instance
+DEDUP_ENTRIES = 1 << 21  # dedupTableSize of BASELINE config 2 (2M entries, 64 MB here)
 QUEUE_BYTES = 3000 << 20
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes (read + write) per expanded node of the search kernel, from an ncu capture of a
-# config-1 batch of 64 instances (1.18 GB for 1.86 M nodes); the bench scales it by the nodes
-# of its own launches, since its workload is too large to capture under ncu.
-NCU_DRAM_BYTES_PER_NODE = 1440.0  # one config-2 m=8 case, profiles/search_engine_config2_single_m8.md
+EXTRAS = ("table_2p30", "learned", "dropin", "reference_gpu", "atomics", "pi_filter")
 
 
 def parse_args():
@@ -44,21 +55,34 @@ def parse_args():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
-    p.add_argument("--batch", type=int, default=40)
+    p.add_argument("--batch", type=int, default=4,
+                   help="cases per step (the 2M-entry table makes an m = 8 case take seconds)")
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--cpu-budget-s", type=float, default=15.0, help="CPU baseline sample length")
+    p.add_argument("--ref-step-s", type=float, default=6.0, help="--impl reference: CPU sample length per step")
     p.add_argument("--cpu-node-limit", type=int, default=3_000_000)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--extras", default=",".join(EXTRAS), help="comma list of extra measurements ('' for none)")
     p.add_argument("--workload", choices=["config2", "config1", "canonical"], default="config2",
                    help="config1 (m~U{4,5,6}) is the small case used for profiling; canonical measures the "
                         "batched canonical form (Configuration.getCanonical) instead of the search")
     p.add_argument("--canonical-count", type=int, default=1_000_000)
     p.add_argument("--table-entries", type=int, default=DEDUP_ENTRIES)
+    p.add_argument("--table-replacement", type=int, default=2)
     p.add_argument("--time-limit-s", type=float, default=600.0)
     p.add_argument("--blocks-per-sm", type=int, default=0, help="engine occupancy cap (0: the kernel's maximum)")
     p.add_argument("--poll-interval", type=int, default=0, help="engine poll interval in chunks (0: the default)")
-    return p.parse_args()
+    p.add_argument("--learned-pairs", type=int, default=400_000)
+    p.add_argument("--learned-eval", type=int, default=20_000)
+    p.add_argument("--ref-budget-s", type=float, default=90.0, help="time budget of each reference_gpu leg")
+    p.add_argument("--ref-case-limit-s", type=float, default=15.0, help="per-case limit of the reference kernel")
+    args = p.parse_args()
+    args.extras = [e for e in args.extras.split(",") if e]
+    unknown = set(args.extras) - set(EXTRAS)
+    if unknown:
+        p.error(f"unknown extras {sorted(unknown)}")
+    return args
 
 
 def dist_env():
@@ -188,16 +212,334 @@ def measured_hbm():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-def algorithmic_bytes(stats, instances: int) -> float:
-    """Bytes the search must move per launch: every transposition-table probe touches a window
-    of 8 entries (8 sectors of 32 B), every insert writes one 32 B entry, every donated task
-    is written and read once (2 x 208 B), every instance is read (144 B) and written (96 B)."""
-    return 256.0 * stats.dedup_probes + 32.0 * stats.dedup_inserts + 416.0 * stats.donations + 240.0 * instances
+ENTRY_BYTES = 32.0  # one transposition-table entry (n <= 32 layout)
+TASK_BYTES = 208.0  # one donated task (written by the donor, read by the receiver)
+INSTANCE_BYTES = 144.0 + 96.0  # InstanceIn read + InstanceOut written
+
+
+def algorithmic_bytes(probes: int, inserts: int, donations: int, instances: int) -> float:
+    """Bytes the search must move: every table probe reads the probed entry (32 B), every
+    insert writes one (32 B), every donated task is written and read once, every instance is
+    read and its result written (the S, E and steal terms of the traffic model)."""
+    return ENTRY_BYTES * probes + ENTRY_BYTES * inserts + 2 * TASK_BYTES * donations + INSTANCE_BYTES * instances
+
+
+STAT_FIELDS = ("nodes", "children", "dedup_probes", "dedup_pruned", "dedup_inserts", "dedup_full", "dedup_replaced",
+               "table_atomics", "donations", "task_pops", "busy_warp_cycles", "warp_cycles", "launches")
+
+
+def set_engine(api, slot, args, **overrides):
+    cfg = api.engine_config(slot)
+    cfg.time_limit_s = args.time_limit_s
+    cfg.table_replacement = args.table_replacement
+    if args.blocks_per_sm > 0:
+        cfg.blocks_per_sm = args.blocks_per_sm
+    if args.poll_interval > 0:
+        cfg.poll_interval = args.poll_interval
+    for k, v in overrides.items():
+        setattr(cfg, k, v)
+    api.set_engine_config(slot, cfg)
+    return cfg
+
+
+def device_steps(lib, api, native, batches, batch, warmup, steps, rate, flush, barrier, clocks=None):
+    """Runs warmup + steps device-resident batches (tdp_batch_prepare outside the timed
+    region, tdp_batch_run timed by the engine's CUDA events).  Returns per-step kernel ms,
+    summed statistics of the timed steps and verdict counts."""
+    kernel_ms, agg, verdicts = [], {f: 0 for f in STAT_FIELDS}, {"found": 0, "not_found": 0, "other": 0}
+    for s in range(warmup + steps):
+        if lib.tdp_batch_prepare(0, batches[s], batch, rate) != 0:
+            raise RuntimeError(native.last_error())
+        flush.fill_(s)
+        barrier()
+        if lib.tdp_batch_run(0) != 0:
+            raise RuntimeError(native.last_error())
+        st = api.last_stats(0)
+        barrier()
+        if s < warmup:
+            continue
+        kernel_ms.append(st.kernel_ms)
+        for f in STAT_FIELDS:
+            agg[f] += getattr(st, f)
+        res = (native.Result * batch)()
+        lib.tdp_batch_results(0, res)
+        for r in res:
+            key = "found" if r.status == native.FOUND else "not_found" if r.status == native.NOT_FOUND else "other"
+            verdicts[key] += 1
+    return kernel_ms, agg, verdicts
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], device="cuda", dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------- extra legs
+def extra_learned(args, api, native):
+    """Plain vs learned root order on two samples, on a slot with a 2^26-entry table: the
+    held-out m = 8..10 set (partial mode, depth 11: every case has a sorting) and full-sorting
+    m = 6..7 configurations at depth 11 (exhaustive negatives among them).  Training pairs
+    come from the plain search in the untimed warm-up; time is the engine's kernel time."""
+    from tdp1375_b200 import learned_eval, order_model
+    from tdp1375_b200.cases import config_cases, MIN_RATE
+    api.GPUSortingSearch(1, 1, QUEUE_BYTES, 1 << 26)
+    try:
+        set_engine(api, 0, args)
+        t0 = time.perf_counter()
+        spi, pi, n, tgt = learned_eval.collect_pairs(0, args.learned_pairs)
+        t_pairs = time.perf_counter() - t0
+        model = order_model.OrderModel()
+        t0 = time.perf_counter()
+        tstats = order_model.train(model, spi, pi, n, tgt, epochs=4, batch=4096, lr=1e-3)
+        t_train = time.perf_counter() - t0
+        if native.load().tdp_mlp_error() != 0:
+            raise RuntimeError("tensor-core wait timed out during training")
+        model.install(0, enable=False)
+        samples = {}
+        held_out = learned_eval.eval_cases(args.learned_eval)
+        stream = [c for c in config_cases(2, 3000) if c[3] in (6, 7)][:400]
+        exhaustive = [c[:3] for c in stream]
+        for name, cases, full in (("held_out_m8_10_partial", held_out, False),
+                                  ("full_sorting_m6_7", exhaustive, True)):
+            out = {"cases": len(cases), "full_sorting": full, "max_depth": MAX_DEPTH}
+            statuses = {}
+            for mode, levels in (("plain", 0), ("learned", 1), ("learned_two_levels", 2)):
+                if native.load().tdp_enable_order_model(0, levels) != 0:
+                    raise RuntimeError(native.last_error())
+                ms, nodes, st = 0.0, 0, []
+                for off in range(0, len(cases), 10000):
+                    part = cases[off:off + 10000]
+                    res = api.search_batch(0, api.make_instances(part, MAX_DEPTH, full), len(part), float(MIN_RATE))
+                    ms += api.last_stats(0).kernel_ms
+                    nodes += sum(r.nodes for r in res[:len(part)])
+                    st += [r.status for r in res[:len(part)]]
+                statuses[mode] = st
+                out[mode] = {"cases_per_s": round(len(cases) / (ms / 1e3), 1), "nodes": nodes,
+                             "kernel_ms": round(ms, 3)}
+            out["verdicts_identical"] = statuses["plain"] == statuses["learned"] == statuses["learned_two_levels"]
+            out["found"] = statuses["plain"].count(native.FOUND)
+            out["not_found"] = statuses["plain"].count(native.NOT_FOUND)
+            for mode in ("learned", "learned_two_levels"):
+                out[mode]["node_ratio_plain_over_this"] = round(out["plain"]["nodes"] / max(1, out[mode]["nodes"]), 3)
+                out[mode]["speedup_over_plain"] = round(out["plain"]["kernel_ms"] / max(1e-9, out[mode]["kernel_ms"]), 3)
+            samples[name] = out
+        native.load().tdp_enable_order_model(0, 0)
+        return {"model": "1088-256-256-256-4960 BF16 MLP, tcgen05 GEMMs; 'learned' reorders each root's children, "
+                         "'learned_two_levels' also the children of each root's 16 best children",
+                "training": {"pairs": int(len(tgt)), "pair_generation_s": round(t_pairs, 2),
+                             "train_s": round(t_train, 2), "steps": tstats.steps,
+                             "loss": [round(tstats.first_loss, 3), round(tstats.last_loss, 3)]},
+                "samples": samples,
+                "note": "time is the engine's kernel time (features, GEMMs, score sorts and search on the slot "
+                        "stream); the model only permutes children, so verdicts must be identical"}
+    finally:
+        api.GPUSortingSearch.destroySlots()
+
+
+def staged_depths(spi, rate):
+    """SortOrExtend.searchForSorting's stages: 4, then min(ub, 8) if ub > 4, then
+    min(ub, 11) if ub > 8, with ub = floor(3-norm * (2 / minRate)) (SortOrExtend.java:89-104)."""
+    from tdp1375_b200.frontier import upper_bound
+    ub = upper_bound(spi, rate)
+    stages = [4]
+    if ub > 4:
+        stages.append(min(ub, 8))
+    if ub > 8:
+        stages.append(min(ub, MAX_DEPTH))
+    return stages
+
+
+def extra_dropin(args, api, native):
+    """One configuration per tdp_search call (the JNI searchForSortingSeq path), staged as
+    SortOrExtend does, over the 673 configurations of the reference's cases-comb.txt."""
+    import ctypes
+    import numpy as np
+    from tdp1375_b200.cases import MIN_RATE
+    recs = json.load(open(os.path.join(ROOT, "tests", "golden", "cases_comb.json")))["records"]
+    lib = native.load()
+    api.GPUSortingSearch(1, 1, QUEUE_BYTES, args.table_entries)
+    try:
+        set_engine(api, 0, args)
+        pos = (ctypes.c_int32 * 48)()
+        depth = ctypes.c_int32(0)
+        lat, found, calls = [], 0, 0
+        rate = ctypes.c_float(float(MIN_RATE))
+        prepared = []
+        for r in recs:
+            spi, pi = r["spi"], r["pi"]
+            n = len(spi)
+            even = sum(1 for c in _cycles(spi) if len(c) % 2 == 1)
+            prepared.append(((ctypes.c_uint8 * n)(*pi), (ctypes.c_uint8 * n)(*spi), n, even,
+                             staged_depths(spi, MIN_RATE)))
+        for _ in range(2):  # warm-up pass over the first configurations
+            for p8, s8, n, even, stages in prepared[:20]:
+                lib.tdp_search(0, p8, s8, n, even, rate, stages[0], 0, pos, ctypes.byref(depth))
+        t_all = time.perf_counter()
+        for p8, s8, n, even, stages in prepared:
+            for d in stages:
+                t0 = time.perf_counter()
+                rc = lib.tdp_search(0, p8, s8, n, even, rate, d, 0, pos, ctypes.byref(depth))
+                lat.append(time.perf_counter() - t0)
+                calls += 1
+                if rc < 0:
+                    raise RuntimeError(native.last_error())
+                if rc == native.FOUND:
+                    found += 1
+                    break
+        wall = time.perf_counter() - t_all
+        lat_ms = np.array(lat) * 1e3
+        return {"configurations": len(prepared), "found": found, "calls": calls,
+                "configurations_per_s": round(len(prepared) / wall, 1), "calls_per_s": round(calls / wall, 1),
+                "call_ms_p50": round(float(np.percentile(lat_ms, 50)), 3),
+                "call_ms_p99": round(float(np.percentile(lat_ms, 99)), 3),
+                "table_entries": args.table_entries,
+                "note": "host-buffer calls (tdp_search) through the C ABI, one slot, partial mode, staged depths "
+                        "4 -> 8 -> 11 as SortOrExtend.searchForSorting (SortOrExtend.java:89-111)"}
+    finally:
+        api.GPUSortingSearch.destroySlots()
+
+
+def _cycles(spi):
+    seen, out = set(), []
+    for x in range(len(spi)):
+        if x in seen:
+            continue
+        c, y = [x], spi[x]
+        seen.add(x)
+        while y != x:
+            c.append(y)
+            seen.add(y)
+            y = spi[y]
+        out.append(c)
+    return out
+
+
+def extra_reference_gpu(args, step0_cases, ours_step_cases_per_s):
+    """The reference's own CUDA search (oracle/_ref, built from the reference sources), one
+    performGpuSortingSearch call per case like GPUSortingSearch: the first headline step's
+    cases (2M-entry table, 3000 MB queue budget, one slot) and SortOrExtend's drop-in calls
+    on cases-comb.txt, each leg within a time budget and a per-case limit."""
+    from oracle import reference_gpu as R
+    from tdp1375_b200.cases import MIN_RATE
+    if not R.available():
+        return {"unavailable": "oracle/_ref/libtdp_ref.so is not built (make -C oracle ref)"}
+    rate = float(MIN_RATE)
+    out = {"source": "reference sorting_search.cu + slot_manager.cu compiled for sm_100a (oracle/Makefile ref)",
+           "table_entries": DEDUP_ENTRIES, "queue_bytes": QUEUE_BYTES, "case_limit_s": args.ref_case_limit_s}
+    R.init(1, 1, QUEUE_BYTES, DEDUP_ENTRIES)
+    try:
+        t0 = time.perf_counter()
+        counts = {"found": 0, "not_found": 0, "timeout": 0, "overflow": 0}
+        tried = 0
+        for pi, spi, even, m in step0_cases:
+            if time.perf_counter() - t0 > args.ref_budget_s:
+                break
+            st, _, _ = R.search(list(pi), list(spi), even, rate, MAX_DEPTH, True, timeout_s=args.ref_case_limit_s)
+            counts[R.STATUS_NAME[st]] += 1
+            tried += 1
+        wall = time.perf_counter() - t0
+        resolved = counts["found"] + counts["not_found"]
+        out["config2_step0"] = {"cases_tried": tried, **counts, "wall_s": round(wall, 2),
+                                "cases_resolved_per_s": round(resolved / wall, 4),
+                                "ours_cases_per_s_same_step": round(ours_step_cases_per_s, 3)}
+        if resolved:
+            out["config2_step0"]["ratio_ours_over_reference"] = round(ours_step_cases_per_s / (resolved / wall), 1)
+        recs = json.load(open(os.path.join(ROOT, "tests", "golden", "cases_comb.json")))["records"]
+        t0 = time.perf_counter()
+        lat, done, found = [], 0, 0
+        for r in recs:
+            if time.perf_counter() - t0 > args.ref_budget_s:
+                break
+            even = sum(1 for c in _cycles(r["spi"]) if len(c) % 2 == 1)
+            for d in staged_depths(r["spi"], MIN_RATE):
+                st, _, ms = R.search(r["pi"], r["spi"], even, rate, d, False, timeout_s=args.ref_case_limit_s)
+                lat.append(ms)
+                if st == R.FOUND:
+                    found += 1
+                    break
+                if st != R.NOT_FOUND:
+                    break
+            done += 1
+        wall = time.perf_counter() - t0
+        import numpy as np
+        out["dropin"] = {"configurations": done, "found": found, "calls": len(lat),
+                         "configurations_per_s": round(done / wall, 2),
+                         "call_ms_p50": round(float(np.percentile(lat, 50)), 2) if lat else None,
+                         "call_ms_p99": round(float(np.percentile(lat, 99)), 2) if lat else None}
+    finally:
+        R.destroy()
+    return out
+
+
+def extra_atomics(native, agg, device_s):
+    import ctypes
+    lib = native.load()
+    peak = ctypes.c_double(0.0)
+    if lib.tdp_measure_atomics(DEDUP_ENTRIES, 1, 2048, ctypes.byref(peak)) != 0:
+        return {"unavailable": lib.tdp_measure_last_error().decode()}
+    achieved = agg["table_atomics"] / device_s
+    return {"achieved": round(achieved, 1), "peak": round(peak.value, 1), "unit": "atomics/s",
+            "frac": round(achieved / peak.value, 6),
+            "per_step": round(agg["table_atomics"] / max(1, agg["launches"]), 1),
+            "note": "engine: transposition-table claims and best-depth updates (table_atomics) over kernel time; "
+                    "peak: returning 32-bit atomicCAS at random entries of a 64 MB (2M x 32 B, L2-resident) "
+                    "buffer from 8 blocks x 256 threads per SM (tdp_measure_atomics), measured in this run"}
+
+
+PI_FILTER_CASES = [(11, [0, 4, 1, 7, 3, 9, 2], [1, 7, 9]), (12, [2, 5, 9, 0, 7, 3, 11], [5, 0, 3])]
+
+
+def extra_pi_filter(native):
+    """tdp_pi_filter (host buffers, every (n-1)! candidate with pi[0] = 0) at n = 11 and 12:
+    kernel time from CUDA events and wall time of the call, beside the reference's
+    performGpuPiFilter on the same input (wall time of its host call; it keeps at most
+    1,048,576 rows).  Both with the 2-move check."""
+    import ctypes
+    from oracle import reference_gpu as R
+    lib = native.load()
+    out = {}
+    for n, cycle, triple in PI_FILTER_CASES:
+        total = 1
+        for i in range(2, n):
+            total *= i
+        c8 = (ctypes.c_uint8 * len(cycle))(*cycle)
+        t8 = (ctypes.c_uint8 * len(triple))(*triple)
+        max_rows = 1 << 20
+        rows = (ctypes.c_uint8 * (max_rows * n))()
+        lib.tdp_pi_filter(c8, len(cycle), t8, len(triple), n, 0, rows, max_rows)  # warm-up
+        kms, walls = [], []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            hits = lib.tdp_pi_filter(c8, len(cycle), t8, len(triple), n, 0, rows, max_rows)
+            walls.append(time.perf_counter() - t0)
+            kms.append(lib.tdp_pi_filter_last_kernel_ms())
+            if hits < 0:
+                raise RuntimeError(native.last_error())
+        k = min(kms)
+        rec = {"candidates": total, "hits": int(hits), "kernel_ms": round(k, 3),
+               "candidates_per_s": round(total / (k / 1e3), 1), "call_ms": round(min(walls) * 1e3, 3)}
+        if R.available():
+            R.pi_filter(cycle, triple, n, False)  # warm-up
+            rw = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                ref_rows = R.pi_filter(cycle, triple, n, False)
+                rw.append(time.perf_counter() - t0)
+            rec["reference_call_ms"] = round(min(rw) * 1e3, 3)
+            rec["reference_rows"] = len(ref_rows)
+            rec["call_speedup_over_reference"] = round(min(rw) / min(walls), 2)
+        out[f"n{n}"] = rec
+    out["note"] = ("kernel_ms: count, scan and write kernels of tdp_pi_filter (packed 4-bit registers, n <= 16); "
+                   "call_ms includes its allocations and copies, like reference_call_ms (performGpuPiFilter, "
+                   "oracle/_ref); the filter is ALU-bound (candidates generated on chip, hits written)")
+    return out
 
 
 def run_ours(args):
-    import ctypes
-
     import torch
 
     rank, world, local = dist_env()
@@ -205,6 +547,7 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     torch.cuda.set_device(local)
+    import numpy as np
     from tdp1375_b200 import GPUSortingSearch, api, make_instances, native
 
     lib = native.load()
@@ -212,90 +555,50 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(args.cpu_budget_s, args.cpu_node_limit)
 
-    GPUSortingSearch(1, 1, QUEUE_BYTES, args.table_entries)  # slot 0 on the current device
-    cfg = api.engine_config(0)
-    cfg.time_limit_s = args.time_limit_s
-    if args.blocks_per_sm > 0:
-        cfg.blocks_per_sm = args.blocks_per_sm
-    if args.poll_interval > 0:
-        cfg.poll_interval = args.poll_interval
-    api.set_engine_config(0, cfg)
     config_id = 1 if args.workload == "config1" else CONFIG
     flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")
     total_steps = args.warmup + args.steps
-
-    batches = [make_instances([c[:3] for c in step_cases(s, rank, world, args.batch, config_id)], MAX_DEPTH, True)
-               for s in range(total_steps)]
-    rate = ctypes.c_float(float(__import__("numpy").float32(2) / __import__("numpy").float32(1.375)))
+    raw_steps = [step_cases(s, rank, world, args.batch, config_id) for s in range(total_steps)]
+    batches = [make_instances([c[:3] for c in cases], MAX_DEPTH, True) for cases in raw_steps]
+    rate = __import__("ctypes").c_float(float(np.float32(2) / np.float32(1.375)))
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    # ---- device-resident value
-    kernel_ms = []
-    stats = []
-    found = notfound = other = 0
+    # ---- device-resident value on the BASELINE table
+    GPUSortingSearch(1, 1, QUEUE_BYTES, args.table_entries)  # slot 0 on the current device
+    cfg = set_engine(api, 0, args)
     with ClockSampler(local) as clocks:
-        for s in range(total_steps):
-            if lib.tdp_batch_prepare(0, batches[s], args.batch, rate) != 0:
-                raise RuntimeError(native.last_error())
-            flush.fill_(s)
-            barrier()
-            if lib.tdp_batch_run(0) != 0:
-                raise RuntimeError(native.last_error())
-            st = api.last_stats(0)
-            barrier()
-            if s >= args.warmup:
-                kernel_ms.append(st.kernel_ms)
-                stats.append((st.nodes, st.children, st.dedup_probes, st.dedup_inserts, st.donations, st.launches,
-                              st.busy_warp_cycles, st.warp_cycles))
-                res = (native.Result * args.batch)()
-                lib.tdp_batch_results(0, res)
-                for r in res:
-                    if r.status == native.FOUND:
-                        found += 1
-                    elif r.status == native.NOT_FOUND:
-                        notfound += 1
-                    else:
-                        other += 1
-    device_s = sum(kernel_ms) / 1e3
-    if world > 1:
-        t = torch.tensor([device_s], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        device_s = float(t.item())
+        kernel_ms, agg, verdicts = device_steps(lib, api, native, batches, args.batch, args.warmup, args.steps, rate,
+                                                flush, barrier)
+    device_s = max_over_ranks(sum(kernel_ms) / 1e3, world)
     cases = args.batch * args.steps * world
     value = cases / device_s
-    nodes = sum(x[0] for x in stats)
+    nodes = agg["nodes"]
 
-    # ---- e2e through the C ABI with host buffers
+    # ---- e2e through the C ABI with host buffers, on the same timed steps (the engine is warm)
     wall = 0.0
     results = (native.Result * args.batch)()
-    for s in range(0 if args.no_e2e else total_steps):
+    for s in range(args.warmup, args.warmup if args.no_e2e else total_steps):
         flush.fill_(s)
         barrier()
         t0 = time.perf_counter()
         if lib.tdp_search_batch(0, batches[s], args.batch, rate, results) != 0:
             raise RuntimeError(native.last_error())
-        dt = time.perf_counter() - t0
+        wall += time.perf_counter() - t0
         barrier()
-        if s >= args.warmup:
-            wall += dt
-    if world > 1:
-        t = torch.tensor([wall], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        wall = float(t.item())
+    wall = max_over_ranks(wall, world)
+    GPUSortingSearch.destroySlots()
 
-    # ---- roofline of the search kernel (per launch averages over the timed steps)
-    class S:  # aggregate stats as an object for algorithmic_bytes
-        dedup_probes = sum(x[2] for x in stats)
-        dedup_inserts = sum(x[3] for x in stats)
-        donations = sum(x[4] for x in stats)
-    launches = sum(x[5] for x in stats)
-    bytes_total = algorithmic_bytes(S, args.batch * args.steps)
+    # ---- roofline of the search kernel (per launch, averaged over the timed steps)
+    launches = max(1, agg["launches"])
+    bytes_total = algorithmic_bytes(agg["dedup_probes"], agg["dedup_inserts"], agg["donations"],
+                                    args.batch * args.steps)
     peak, peak_kind = measured_hbm()
-    achieved = bytes_total / device_s / 1e9
+    mean_launch_s = (sum(kernel_ms) / 1e3) / launches
+    achieved = bytes_total / launches / mean_launch_s / 1e9
     line = {
         "metric": "cases resolved/s (config-2 3-permutations, full sorting, ratio 1.375, depth 11)",
         "value": round(value, 3),
@@ -312,30 +615,54 @@ def run_ours(args):
         "config": {"workload": ("config2: 100,000 seeded 3-permutations, m~U{4..8} (n<=24)" if config_id == 2 else
                                  "config1: seeded 3-permutations, m~U{4,5,6} (n<=18)") +
                                 ", full sorting, ratio 1.375, max depth 11, 3000 MB queue budget, 1 slot",
-                   "table_entries": args.table_entries, "batch_per_step": args.batch, "l2": "flushed by a 256 MB write between steps",
+                   "table_entries": args.table_entries, "batch_per_step": args.batch,
+                   "l2": "flushed by a 256 MB write between steps",
                    "parallelism": f"replicas x{world} (cases sharded, no collective)",
                    "engine": {"blocks_per_sm": cfg.blocks_per_sm, "poll_interval": cfg.poll_interval,
-                              "sparse_enumeration": cfg.sparse_enumeration, "tight_bound": cfg.tight_bound}},
+                              "sparse_enumeration": cfg.sparse_enumeration, "tight_bound": cfg.tight_bound,
+                              "table_replacement": cfg.table_replacement}},
         "nodes_per_s": round(nodes / (sum(kernel_ms) / 1e3), 1),
-        "verdicts": {"found": found, "not_found": notfound, "other": other},
-        "warp_busy_frac": round(sum(x[6] for x in stats) / max(1, sum(x[7] for x in stats)), 4),
-        "gpu_launches": launches,
+        "verdicts": verdicts,
+        "counters_per_step": {f: round(agg[f] / args.steps, 1) for f in STAT_FIELDS if f != "launches"},
+        "warp_busy_frac": round(agg["busy_warp_cycles"] / max(1, agg["warp_cycles"]), 4),
+        "gpu_launches": agg["launches"],
         "roofline": {"bound": "hbm", "achieved": round(achieved, 3), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 6),
-                     "traffic": round(NCU_DRAM_BYTES_PER_NODE * nodes / launches, 1) if launches else None,
-                     "note": f"algorithmic table/task/instance bytes over kernel time; peak {peak_kind}; traffic = "
-                             "DRAM bytes per launch scaled from an ncu capture (1.44 kB per expanded node) by the "
-                             "launch's nodes; the kernel is bound by table-probe latency and warp count (ncu: "
-                             "issue-active 47%, DRAM throughput 5.1%, long-scoreboard and fence stalls on top)"},
+                     "frac": round(achieved / peak, 6), "traffic": None,
+                     "note": f"algorithmic bytes per launch = 32 B x (table probes + inserts) + 2 x 208 B x donations "
+                             f"+ 240 B x instances, over the mean launch time (CUDA events on the engine stream); "
+                             f"peak {peak_kind}; the 64 MB table of the BASELINE config stays in L2, so the "
+                             "kernel is bound by table-probe latency and L2 atomics, not HBM bandwidth (see atomics)"},
         "e2e": {"value": round(cases / wall, 3) if wall > 0 else None, "unit": "cases/s",
                 "h2d_bytes_per_step": args.batch * 144, "d2h_bytes_per_step": args.batch * 96},
         "clocks": clocks.summary(),
     }
+    if rank == 0 and world == 1:
+        first_step_ms = kernel_ms[0] if kernel_ms else 0.0
+        if "atomics" in args.extras:
+            line["atomics"] = extra_atomics(native, agg, sum(kernel_ms) / 1e3)
+        if "pi_filter" in args.extras:
+            line["pi_filter"] = extra_pi_filter(native)
+        if "table_2p30" in args.extras:
+            GPUSortingSearch(1, 1, QUEUE_BYTES, 1 << 30)
+            set_engine(api, 0, args)
+            k = min(args.steps, 5)
+            ms2, agg2, v2 = device_steps(lib, api, native, batches, args.batch, 1, k, rate, flush, barrier)
+            GPUSortingSearch.destroySlots()
+            line["table_2p30"] = {"table_entries": 1 << 30, "steps": k, "cases_per_s": round(args.batch * k / (sum(ms2) / 1e3), 3),
+                                  "nodes_per_s": round(agg2["nodes"] / (sum(ms2) / 1e3), 1), "verdicts": v2,
+                                  "note": "the headline's first timed steps on a 32 GB table (labelled extra, not "
+                                          "the BASELINE configuration)"}
+        if "learned" in args.extras:
+            line["learned"] = extra_learned(args, api, native)
+        if "dropin" in args.extras:
+            line["dropin"] = extra_dropin(args, api, native)
+        if "reference_gpu" in args.extras:
+            ours_step = args.batch / (first_step_ms / 1e3) if first_step_ms else 0.0
+            line["reference_gpu"] = extra_reference_gpu(args, raw_steps[args.warmup], ours_step)
     if cpu is not None:
         line["cpu_baseline"] = {"value": round(cpu[0], 4), "unit": "cases/s", "cores": cpu[2], "kind": "port",
                                 "sample": cpu[3], "nodes_per_s": round(cpu[1], 1),
                                 "value_upper_bound": round(cpu[4], 4)}
-    GPUSortingSearch.destroySlots()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -349,7 +676,7 @@ def run_reference(args):
     samples = []
     first = 0
     for s in range(args.warmup + args.steps):
-        cps, nps, cores, detail, _ = cpu_sample(args.cpu_budget_s, args.cpu_node_limit, first_case=first)
+        cps, nps, cores, detail, _ = cpu_sample(args.ref_step_s, args.cpu_node_limit, first_case=first)
         first += 4 * cores
         if s >= args.warmup:
             samples.append((cps, nps))
@@ -362,7 +689,7 @@ def run_reference(args):
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": round(args.cpu_budget_s * 1e3, 1),
+        "ms_per_step": round(args.ref_step_s * 1e3, 1),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,

@@ -187,8 +187,9 @@ int tdp_extension_filter_device(const uint8_t *spi, const uint8_t *pi, int n, in
 /* ---- learned move ordering (no counterpart in the reference) ------------------------
  * A 1088 -> 256 -> 256 -> 256 -> 4960 BF16 MLP (fp32 accumulation on the tcgen05 tensor
  * cores) scores the (i,j,k) triples of a configuration with n <= 32; the batched search then
- * expands each instance's root children in descending score order.  Ordering only permutes
- * children: verdicts are unchanged.  The entry points below take DEVICE pointers and a
+ * expands each instance's root children (and, with two levels, the first level's best
+ * children) in descending score order.  Ordering only permutes children: verdicts are
+ * unchanged.  The entry points below take DEVICE pointers and a
  * cudaStream_t (as void*); they are the building blocks of inference and training. */
 #define TDP_MLP_FEATURES 1088
 #define TDP_MLP_HIDDEN 256
@@ -214,8 +215,11 @@ int tdp_mlp_order(const float *scores, int ld, const uint8_t *n, int count, uint
 int tdp_mlp_error(void);
 
 /* Installs the ordering model on a slot (host arrays: bf16 weights as uint16 bits in the
- * torch.nn.Linear [out, in] layout, fp32 biases; w4 has 4960 rows).  enable = 0 keeps the
- * weights but searches in plain order. */
+ * torch.nn.Linear [out, in] layout, fp32 biases; w4 has 4960 rows).  tdp_enable_order_model
+ * sets how many levels it orders: 0 keeps the weights but searches in plain order; 1 orders
+ * each root's children; 2 also scores the states after each root's 16 best children and
+ * expands each one's 32 best-scoring children first (then all of its children in plain
+ * order, so the search stays exhaustive). */
 int tdp_set_order_model(int slot, const uint16_t *w1, const float *b1, const uint16_t *w2, const float *b2,
                         const uint16_t *w3, const float *b3, const uint16_t *w4, const float *b4);
 int tdp_enable_order_model(int slot, int enable);

@@ -355,8 +355,9 @@ int tdp_set_order_model(int slot, const uint16_t *w1, const float *b1, const uin
 int tdp_enable_order_model(int slot, int enable) {
     auto s = get_slot(slot);
     if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
+    if (enable < 0 || enable > 2) return fail(TDP_ERR_ARGUMENT, "tdp_enable_order_model: levels must be 0, 1 or 2");
     if (enable && !s->hasOrderModel()) return fail(TDP_ERR_ARGUMENT, "tdp_enable_order_model: no model installed");
-    s->enableOrderModel(enable != 0);
+    s->enableOrderModel(enable);
     return 0;
 }
 

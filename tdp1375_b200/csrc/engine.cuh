@@ -51,7 +51,7 @@ struct alignas(16) Task {
     uint8_t reserved1;
     uint16_t lo;
     uint16_t hi;
-    uint32_t flags;
+    uint32_t flags;                  // bit 0: unexpanded node; bits 8..15: first-level rank + 1
     uint32_t path[16];
     uint8_t spi[64];
     uint8_t pi[64];
@@ -104,6 +104,11 @@ enum EngineError : int {
     kErrDeadline = 2,
 };
 
+// Learned order below the root: the best kLevel1Ranks root children each get a list of
+// their kLevel1List best children, expanded first.
+constexpr int kLevel1Ranks = 16;
+constexpr int kLevel1List = 32;
+
 constexpr uint32_t kTagWriting = 0xFFFFFFFFu;
 constexpr uint32_t kMaxGeneration = 4094;  // generation 4095 would collide with kTagWriting
 constexpr int kInstanceBits = 20;          // up to 1,048,576 instances per launch
@@ -148,6 +153,9 @@ struct EngineParams {
     int sparse;                      // same-cycle pair enumeration allowed (n <= 32)
     const uint16_t *order;           // per-instance root child order (learned), or null
     int orderStride;
+    const uint16_t *order2;          // per (instance, root rank < order2Ranks): best children of
+                                     // that first-level node, order2List entries, or null
+    int order2Ranks, order2List;
     int maxInFlight;                 // admitted-but-unfinished instance cap (0 = none)
     int replace;                     // full-window policy: 0 admit unrecorded, 1 deepest, 2 oldest,
                                      // 3 deepest then oldest (see dedup_admit)

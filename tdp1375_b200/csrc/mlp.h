@@ -49,6 +49,14 @@ void adam_step(float *master, __nv_bfloat16 *weight, const float *grad, float *m
 // Per instance: the n-space lexicographic triple indices ordered by descending score.
 void order_by_score(const float *scores, int ld, const uint8_t *n, int nStride, int count, uint16_t *order,
                     int orderStride, cudaStream_t stream);
+// States after the first k1 children of each instance's root order: rows s*k1 + r of
+// outSpi/outPi (64 bytes) and outN (0 when the root has fewer than r + 1 triples).
+void level1_states(const uint8_t *spi, const uint8_t *pi, const uint8_t *n, int rowStride, int nStride, int count,
+                   const uint16_t *order, int orderStride, int k1, uint8_t *outSpi, uint8_t *outPi, uint8_t *outN,
+                   cudaStream_t stream);
+// Per state: the k best-scoring n-space triple indices, best first (0xFFFF past the triples).
+void top_k(const float *scores, int ld, const uint8_t *n, int nStride, int count, int k, uint16_t *out, int outStride,
+           cudaStream_t stream);
 
 }  // namespace mlp
 }  // namespace tdp

@@ -226,6 +226,114 @@ __global__ void __launch_bounds__(1024) order_kernel(const float *scores, int ld
     for (int t = threadIdx.x; t < T; t += blockDim.x) order[(size_t)s * orderStride + t] = val[t];
 }
 
+// First-level states of the learned order: for instance s and rank r < K1 of its root
+// order, the state after the root child order[r] (positions i<j<k of the root's pi array):
+// spi' = spi o (a b c)^-1 with a, b, c = pi[i], pi[j], pi[k] (sorting_search.cu:543-555) and
+// pi' = pi with [i,j) and [j,k) swapped (transposition.cuh:5-19).  Ranks past the root's
+// triple count get n = 0.
+__global__ void level1_states_kernel(const uint8_t *spi, const uint8_t *pi, const uint8_t *nArr, int rowStride,
+                                     int nStride, int count, const uint16_t *order, int orderStride, int k1,
+                                     uint8_t *outSpi, uint8_t *outPi, uint8_t *outN) {
+    const int row = blockIdx.x;  // s * k1 + r
+    const int s = row / k1, r = row % k1;
+    if (s >= count) return;
+    const int n = min((int)nArr[(size_t)s * nStride], 32);
+    const int T = combinations3(n);
+    const int p = threadIdx.x;  // 32 threads: one position / symbol each
+    __shared__ int ijk[3];
+    if (p == 0) {
+        int rem = (r < T) ? (int)order[(size_t)s * orderStride + r] : 0, i = 0;
+        while (i < n - 3 && rem >= (n - 1 - i) * (n - 2 - i) / 2) rem -= (n - 1 - i) * (n - 2 - i) / 2, ++i;
+        int j = i + 1;
+        while (j < n - 2 && rem >= n - 1 - j) rem -= n - 1 - j, ++j;
+        ijk[0] = i;
+        ijk[1] = j;
+        ijk[2] = j + 1 + rem;
+    }
+    __syncthreads();
+    const uint8_t *sp = spi + (size_t)s * rowStride, *pp = pi + (size_t)s * rowStride;
+    uint8_t *os = outSpi + (size_t)row * 64, *op = outPi + (size_t)row * 64;
+    const bool valid = r < T;
+    if (p == 0) outN[row] = valid ? (uint8_t)n : (uint8_t)0;
+    if (!valid || p >= n) {
+        if (p < 32) os[p] = op[p] = 0;
+        return;
+    }
+    const int i = ijk[0], j = ijk[1], k = ijk[2];
+    const int a = pp[i], b = pp[j], c = pp[k];
+    uint8_t v = sp[p];
+    if (p == a) v = sp[c];
+    if (p == b) v = sp[a];
+    if (p == c) v = sp[b];
+    os[p] = v;
+    op[p] = pp[block_swap_src(p, i, j, k)];
+}
+
+// The K highest-scoring triples of each state (n-space lexicographic indices, ties to the
+// smaller index, the order of order_kernel), by K rounds of a block arg-max; 0xFFFF pads
+// states with fewer than K triples.
+__global__ void __launch_bounds__(256) topk_kernel(const float *scores, int ld, const uint8_t *nArr, int nStride,
+                                                   int count, int k, uint16_t *out, int outStride) {
+    constexpr int kPer = 20;  // 256 * 20 >= C(32,3) = 4960
+    const int s = blockIdx.x;
+    if (s >= count) return;
+    const int n = min((int)nArr[(size_t)s * nStride], 32);
+    const int T = combinations3(n);
+    float key[kPer];
+#pragma unroll
+    for (int e = 0; e < kPer; ++e) {
+        const int t = threadIdx.x + 256 * e;
+        key[e] = -FLT_MAX;
+        if (t < T) {
+            int rem = t, i = 0;
+            while (i < n - 3 && rem >= (n - 1 - i) * (n - 2 - i) / 2) rem -= (n - 1 - i) * (n - 2 - i) / 2, ++i;
+            int j = i + 1;
+            while (j < n - 2 && rem >= n - 1 - j) rem -= n - 1 - j, ++j;
+            key[e] = scores[(size_t)s * ld + lex32(i, j, j + 1 + rem)];
+        }
+    }
+    unsigned taken = 0;
+    __shared__ float bestKey[8];
+    __shared__ int bestIdx[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int round = 0; round < k; ++round) {
+        float bk = -FLT_MAX;
+        int bi = 0x7FFFFFFF;
+#pragma unroll
+        for (int e = 0; e < kPer; ++e) {
+            const int t = threadIdx.x + 256 * e;
+            if (t < T && !((taken >> e) & 1u) && (key[e] > bk || (key[e] == bk && t < bi))) {
+                bk = key[e];
+                bi = t;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ok = __shfl_xor_sync(0xFFFFFFFFu, bk, o);
+            const int oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
+            if (ok > bk || (ok == bk && oi < bi)) {
+                bk = ok;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            bestKey[warp] = bk;
+            bestIdx[warp] = bi;
+        }
+        __syncthreads();
+        bk = bestKey[0];
+        bi = bestIdx[0];
+        for (int w = 1; w < 8; ++w)
+            if (bestKey[w] > bk || (bestKey[w] == bk && bestIdx[w] < bi)) {
+                bk = bestKey[w];
+                bi = bestIdx[w];
+            }
+        __syncthreads();
+        if (threadIdx.x == 0) out[(size_t)s * outStride + round] = bi < T ? (uint16_t)bi : (uint16_t)0xFFFF;
+        if (bi < T && (bi & 255) == (int)threadIdx.x) taken |= 1u << (bi >> 8);
+    }
+}
+
 }  // namespace
 
 void build_features(const uint8_t *spi, const uint8_t *pi, const uint8_t *n, int rowStride, int nStride, int count,
@@ -260,6 +368,19 @@ void adam_step(float *master, __nv_bfloat16 *weight, const float *grad, float *m
 void order_by_score(const float *scores, int ld, const uint8_t *n, int nStride, int count, uint16_t *order,
                     int orderStride, cudaStream_t stream) {
     if (count > 0) order_kernel<<<count, 1024, 0, stream>>>(scores, ld, n, nStride, count, order, orderStride);
+}
+
+void level1_states(const uint8_t *spi, const uint8_t *pi, const uint8_t *n, int rowStride, int nStride, int count,
+                   const uint16_t *order, int orderStride, int k1, uint8_t *outSpi, uint8_t *outPi, uint8_t *outN,
+                   cudaStream_t stream) {
+    if (count > 0 && k1 > 0)
+        level1_states_kernel<<<count * k1, 32, 0, stream>>>(spi, pi, n, rowStride, nStride, count, order, orderStride,
+                                                            k1, outSpi, outPi, outN);
+}
+
+void top_k(const float *scores, int ld, const uint8_t *n, int nStride, int count, int k, uint16_t *out, int outStride,
+           cudaStream_t stream) {
+    if (count > 0 && k > 0) topk_kernel<<<count, 256, 0, stream>>>(scores, ld, n, nStride, count, k, out, outStride);
 }
 
 }  // namespace mlp

@@ -144,6 +144,10 @@ SearchSlot::~SearchSlot() {
     for (int l = 0; l < 3; ++l) cudaFree(dH_[l]);
     cudaFree(dScores_);
     cudaFree(dOrder_);
+    cudaFree(dOrder2_);
+    cudaFree(dL1Spi_);
+    cudaFree(dL1Pi_);
+    cudaFree(dL1N_);
     cudaFree(dMlpErr_);
     dropGraph();
     cudaFree(dGen_);
@@ -309,6 +313,9 @@ void SearchSlot::launchClass(int cls, int offset, int count) {
     P.sparse = cfg_.sparse_enumeration;
     P.order = (cls == 0 && orderedLaunch_) ? dOrder_ : nullptr;
     P.orderStride = combinations3(32);
+    P.order2 = (cls == 0 && orderedLaunch_ && orderLevels_ >= 2) ? dOrder2_ : nullptr;
+    P.order2Ranks = kLevel1Ranks;
+    P.order2List = kLevel1List;
     P.replace = cfg_.table_replacement;
     P.commute = cfg_.commute;
 
@@ -509,7 +516,9 @@ int SearchSlot::setOrderModel(const uint16_t *w1, const float *b1, const uint16_
 }
 
 // Scores every staged n <= 32 root with the MLP (tensor-core GEMMs on the slot stream, in
-// chunks) and sorts its children by descending score into dOrder_.
+// chunks) and sorts its children by descending score into dOrder_.  With two levels it also
+// builds the states after each root's kLevel1Ranks best children, scores them the same way
+// and keeps each one's kLevel1List best children in dOrder2_.
 constexpr int kOrderChunk = 8192;
 
 // Buffers of the ordering pipeline; allocated before any graph capture.
@@ -520,6 +529,20 @@ void SearchSlot::prepareOrderBuffers(int count) {
         dOrder_ = nullptr;
         check(cudaMalloc(&dOrder_, (size_t)count * stride * sizeof(uint16_t)), "cudaMalloc(order)");
         orderCap_ = count;
+    }
+    if (orderLevels_ >= 2 && count > order2Cap_) {
+        cudaFree(dOrder2_);
+        cudaFree(dL1Spi_);
+        cudaFree(dL1Pi_);
+        cudaFree(dL1N_);
+        dOrder2_ = nullptr;
+        dL1Spi_ = dL1Pi_ = dL1N_ = nullptr;
+        const size_t rows = (size_t)count * kLevel1Ranks;
+        check(cudaMalloc(&dOrder2_, rows * kLevel1List * sizeof(uint16_t)), "cudaMalloc(first-level order)");
+        check(cudaMalloc(&dL1Spi_, rows * 64), "cudaMalloc(first-level states)");
+        check(cudaMalloc(&dL1Pi_, rows * 64), "cudaMalloc(first-level states)");
+        check(cudaMalloc(&dL1N_, rows), "cudaMalloc(first-level states)");
+        order2Cap_ = count;
     }
     if (!dX_) {
         check(cudaMalloc(&dX_, (size_t)kOrderChunk * mlp::kFeatures * 2), "cudaMalloc(features)");
@@ -533,12 +556,10 @@ int SearchSlot::computeRootOrder(int count, std::string &err) {
     constexpr int kChunk = kOrderChunk;
     const int stride = combinations3(32);
     const uint8_t *base = reinterpret_cast<const uint8_t *>(dIn_);
-    for (int off = 0; off < count; off += kChunk) {
-        const int rows = std::min(kChunk, count - off);
-        const uint8_t *rec = base + (size_t)off * sizeof(InstanceIn);
-        mlp::build_features(rec + offsetof(InstanceIn, spi), rec + offsetof(InstanceIn, pi),
-                            rec + offsetof(InstanceIn, n), (int)sizeof(InstanceIn), (int)sizeof(InstanceIn), rows,
-                            static_cast<__nv_bfloat16 *>(dX_), stream_);
+    // features -> 3 hidden layers -> scores for `rows` states; then rank them
+    auto score = [&](const uint8_t *spi, const uint8_t *pi, const uint8_t *n, int rowStride, int nStride,
+                     int rows) -> int {
+        mlp::build_features(spi, pi, n, rowStride, nStride, rows, static_cast<__nv_bfloat16 *>(dX_), stream_);
         const void *in = dX_;
         int k = mlp::kFeatures;
         for (int l = 0; l < 3; ++l) {
@@ -551,8 +572,29 @@ int SearchSlot::computeRootOrder(int count, std::string &err) {
         if (mlp::gemm_bf16(in, dW_[3], rows, mlp::kTriplesPadded, mlp::kHidden, dB_[3], 0, dScores_, 1,
                            mlp::kTriplesPadded, dMlpErr_, stream_, err) != 0)
             return TDP_ERR_CUDA;
+        return 0;
+    };
+    for (int off = 0; off < count; off += kChunk) {
+        const int rows = std::min(kChunk, count - off);
+        const uint8_t *rec = base + (size_t)off * sizeof(InstanceIn);
+        if (score(rec + offsetof(InstanceIn, spi), rec + offsetof(InstanceIn, pi), rec + offsetof(InstanceIn, n),
+                  (int)sizeof(InstanceIn), (int)sizeof(InstanceIn), rows) != 0)
+            return TDP_ERR_CUDA;
         mlp::order_by_score(dScores_, mlp::kTriplesPadded, rec + offsetof(InstanceIn, n), (int)sizeof(InstanceIn),
                             rows, dOrder_ + (size_t)off * stride, stride, stream_);
+    }
+    if (orderLevels_ >= 2) {
+        mlp::level1_states(base + offsetof(InstanceIn, spi), base + offsetof(InstanceIn, pi),
+                           base + offsetof(InstanceIn, n), (int)sizeof(InstanceIn), (int)sizeof(InstanceIn), count,
+                           dOrder_, stride, kLevel1Ranks, dL1Spi_, dL1Pi_, dL1N_, stream_);
+        const int states = count * kLevel1Ranks;
+        for (int off = 0; off < states; off += kChunk) {
+            const int rows = std::min(kChunk, states - off);
+            if (score(dL1Spi_ + (size_t)off * 64, dL1Pi_ + (size_t)off * 64, dL1N_ + off, 64, 1, rows) != 0)
+                return TDP_ERR_CUDA;
+            mlp::top_k(dScores_, mlp::kTriplesPadded, dL1N_ + off, 1, rows, kLevel1List,
+                       dOrder2_ + (size_t)off * kLevel1List, kLevel1List, stream_);
+        }
     }
     check(cudaGetLastError(), "ordering model launch");
     return 0;

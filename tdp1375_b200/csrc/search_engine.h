@@ -57,8 +57,11 @@ public:
     int setOrderModel(const uint16_t *w1, const float *b1, const uint16_t *w2, const float *b2, const uint16_t *w3,
                       const float *b3, const uint16_t *w4, const float *b4, std::string &err);
     bool hasOrderModel() const { return dW_[0] != nullptr; }
-    void enableOrderModel(bool on) {
-        orderEnabled_ = on;
+    // levels: 0 plain order, 1 learned root order, 2 learned root order and learned lists
+    // at the first level below it
+    void enableOrderModel(int levels) {
+        orderEnabled_ = levels > 0;
+        orderLevels_ = levels;
         graphValid_ = false;
     }
 
@@ -110,6 +113,12 @@ private:
     void *dW_[4] = {nullptr, nullptr, nullptr, nullptr};
     float *dB_[4] = {nullptr, nullptr, nullptr, nullptr};
     bool orderEnabled_ = false;
+    int orderLevels_ = 0;
+    // first-level lists: the states after the best kLevel1Ranks root children, scored by the
+    // model, and each one's kLevel1List best children
+    uint8_t *dL1Spi_ = nullptr, *dL1Pi_ = nullptr, *dL1N_ = nullptr;
+    uint16_t *dOrder2_ = nullptr;
+    int order2Cap_ = 0;
     void *dX_ = nullptr, *dH_[3] = {nullptr, nullptr, nullptr};
     float *dScores_ = nullptr;
     uint16_t *dOrder_ = nullptr;

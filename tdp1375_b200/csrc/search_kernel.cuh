@@ -603,6 +603,7 @@ struct WarpShared {
     uint32_t tri[NW == 1 ? kMaxTriples : 1];  // triple list of the frame being enumerated
     uint64_t rules[32];                       // success (0..15) and expansion (16..31) tables of the instance
     unsigned long long taskNodes, taskChildren;  // counters of the task in hand
+    int rank1;                                   // root-order rank of the current first-level node (-1: none)
     uint32_t staging[52];
     unsigned long long stats[kStatCount];  // per-warp counters, flushed once at exit
 };
@@ -708,7 +709,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
             even = (int)((S.staging[1] >> 8) & 0xFFu);
             lo = (int)(S.staging[2] & 0xFFFFu);
             hi = (int)(S.staging[2] >> 16);
-            if (lane == 0) S.taskNodes = S.staging[3] & 1u;
+            if (lane == 0) {
+                S.taskNodes = S.staging[3] & 1u;
+                S.rank1 = baseDepth == 1 ? (int)((S.staging[3] >> 8) & 0xFFu) - 1 : -1;
+            }
             if (lane < baseDepth) S.frames[lane].move = S.staging[4 + lane];
             const uint8_t *bytes = reinterpret_cast<const uint8_t *>(S.staging);
             const int n = P.in[inst].n;
@@ -735,7 +739,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                 const int x = lane + 32 * h;
                 w[h] = (x < n) ? ((uint32_t)I->spi[x] | ((uint32_t)I->pi[x] << 6)) : 0u;
             }
-            if (lane == 0) S.taskNodes = 1;
+            if (lane == 0) {
+                S.taskNodes = 1;
+                S.rank1 = -1;
+            }
         }
         if (lane == 0) S.taskChildren = 0;
         const int n = P.in[inst].n;
@@ -758,12 +765,36 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
         uint64_t satMask = S.rules[f + 1];
         uint64_t expMask = S.rules[16 + f + 1];
         // The root of an instance with a learned order enumerates its children in that order
-        // (dense mode, index space = positions in the order).
+        // (dense mode, index space = positions in the order).  With first-level lists, the
+        // node after root child rank r < order2Ranks enumerates its list first and then every
+        // child in plain order (dense, index space = list slots then triples), so it stays
+        // exhaustive; a child in both parts meets the table the second time.
         const uint16_t *rootOrder = (P.order && NW == 1) ? P.order + (size_t)inst * (size_t)P.orderStride : nullptr;
-        SparseFrame sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, (rootOrder && f == 0) ? 0 : P.sparse, S.tri);
+        auto listOf = [&](int g) -> const uint16_t * {
+            if (!P.order2 || !rootOrder || g != 1) return nullptr;
+            const int r = S.rank1;
+            return (r >= 0 && r < P.order2Ranks) ? P.order2 + ((size_t)inst * P.order2Ranks + r) * P.order2List
+                                                 : nullptr;
+        };
+        auto ordered = [&](int g) -> bool { return (rootOrder && g == 0) || listOf(g) != nullptr; };
+        // dense index t of frame g -> packed triple; 0xFFFFFFFF marks an empty list slot
+        auto decode = [&](int g, int t) -> uint32_t {
+            if (rootOrder && g == 0) return __ldg(trip + (int)__ldg(rootOrder + t));
+            const uint16_t *L = listOf(g);
+            if (L) {
+                if (t < P.order2List) {
+                    const uint16_t e = __ldg(L + t);
+                    return e == 0xFFFFu ? 0xFFFFFFFFu : __ldg(trip + (int)e);
+                }
+                t -= P.order2List;
+            }
+            return __ldg(trip + t);
+        };
+        auto denseEnd = [&](int g) -> int { return T + (listOf(g) ? P.order2List : 0); };
+        SparseFrame sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, ordered(f) ? 0 : P.sparse, S.tri);
         // A donated range is in the units of its frame's mode (the receiver derives the same
         // mode from the same node); hi = 0xFFFF covers every child.
-        if (hi == 0xFFFF) end = sf.mode ? sf.np : T;
+        if (hi == 0xFFFF) end = sf.mode ? sf.np : denseEnd(f);
 
         // outcome: 0 subtree exhausted, 1 instance found (here or elsewhere), 2 launch stop
         int outcome = 0;
@@ -793,8 +824,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                     for (int h = 0; h < NW; ++h) w[h] = S.words[f][h * 32 + lane];
                     satMask = S.rules[f + 1];
                     expMask = S.rules[16 + f + 1];
-                    sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, (rootOrder && f == 0) ? 0 : P.sparse,
-                                          S.tri);
+                    sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, ordered(f) ? 0 : P.sparse, S.tri);
                     continue;
                 }
                 if (++poll >= P.pollInterval) {
@@ -876,8 +906,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                                 const uint64_t gSat = S.rules[g + 1];
                                 const uint64_t gExp = S.rules[16 + g + 1];
                                 const SparseFrame gsf =
-                                    sparse_setup<NW>(wg, n, lane, gEven, gSat, gExp, (rootOrder && g == 0) ? 0 : P.sparse,
-                                                     nullptr);
+                                    sparse_setup<NW>(wg, n, lane, gEven, gSat, gExp, ordered(g) ? 0 : P.sparse, nullptr);
                                 uint32_t ctr;
                                 if (gsf.mode == 1) {
                                     const PairSel ps = sparse_pair(gsf, gChunk);
@@ -888,7 +917,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                                     ctr = triple_at(gsf, gChunk + l);
                                 } else {
                                     const int t = gChunk + l;
-                                    ctr = __ldg(trip + ((rootOrder && g == 0) ? (int)__ldg(rootOrder + t) : t));
+                                    ctr = decode(g, t);
                                 }
                                 const uint32_t ci = tri_i(ctr), cj = tri_j(ctr), ck = tri_k(ctr);
                                 const uint32_t ca = w_pi(gather<NW>(wg, ci));
@@ -913,6 +942,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                                 hdr1 = (uint32_t)(g + 1) | ((uint32_t)cEven << 8);
                                 hdr2 = 0xFFFFu << 16;
                                 hdr3 = 1u;
+                                // a root child handed over keeps its learned rank (first-level list)
+                                if (g == 0 && rootOrder && gChunk + l < P.order2Ranks)
+                                    hdr3 |= (uint32_t)(gChunk + l + 1) << 8;
                                 const uint32_t bit = 1u << l;
                                 if (g == f) {
                                     pending &= ~bit;
@@ -939,6 +971,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                                 hdr1 = (uint32_t)g | ((uint32_t)gEven << 8);
                                 hdr2 = (uint32_t)newEnd | ((uint32_t)ge << 16);
                                 hdr3 = 0u;
+                                // a first-level range is in its list's index space: pass the rank
+                                if (g == 1 && S.rank1 >= 0 && S.rank1 < P.order2Ranks)
+                                    hdr3 |= (uint32_t)(S.rank1 + 1) << 8;
                                 if (g == f) {
                                     end = newEnd;
                                 } else if (lane == 0) {
@@ -1001,7 +1036,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                     if (sf.mode == 2) {
                         tr = valid ? S.tri[t] : 0u;
                     } else {
-                        tr = valid ? __ldg(trip + ((rootOrder && f == 0) ? (int)__ldg(rootOrder + t) : t)) : 0u;
+                        tr = valid ? decode(f, t) : 0u;
+                        if (tr == 0xFFFFFFFFu) {
+                            valid = false;
+                            tr = 0u;
+                        }
                     }
                     a = w_pi(gather<NW>(w, tri_i(tr)));
                     b = w_pi(gather<NW>(w, tri_j(tr)));
@@ -1085,7 +1124,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                 tr = S.tri[chunk + l];
             } else {
                 const int t = chunk + l;
-                tr = __ldg(trip + ((rootOrder && f == 0) ? (int)__ldg(rootOrder + t) : t));
+                tr = decode(f, t);
             }
             if (lane == 0) {
                 FrameRec<KW> &fr = S.frames[f];
@@ -1098,6 +1137,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                 fr.move = tr;
 #pragma unroll
                 for (int q = 0; q < KW; ++q) fr.key[q] = key[q];
+                // leaving the root: the child's rank in the root's learned order
+                if (f == 0) S.rank1 = rootOrder ? chunk + l : -1;
             }
             __syncwarp();
             const uint32_t i = tri_i(tr), j = tri_j(tr), k = tri_k(tr);
@@ -1129,9 +1170,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
             for (int h = 0; h < NW; ++h) S.words[f][h * 32 + lane] = w[h];
             satMask = S.rules[f + 1];
             expMask = S.rules[16 + f + 1];
-            sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, (rootOrder && f == 0) ? 0 : P.sparse, S.tri);
+            sf = sparse_setup<NW>(w, n, lane, even, satMask, expMask, ordered(f) ? 0 : P.sparse, S.tri);
             cursor = 0;
-            end = sf.mode ? sf.np : T;
+            end = sf.mode ? sf.np : denseEnd(f);
             pending = 0u;
             if (lane == 0) ++S.taskNodes;
         }

@@ -162,8 +162,9 @@ class OrderModel:
             self.weight[3][TRIPLES:] = 0.0
         return float(loss.mean()), float(top1)
 
-    def install(self, slot: int, enable: bool = True) -> None:
-        """Copies the weights into the search slot and turns ordering on."""
+    def install(self, slot: int, enable: bool = True, levels: int = 1) -> None:
+        """Copies the weights into the search slot and turns ordering on: levels = 1 orders each
+        root's children, 2 also the first level's (enable = False keeps plain order)."""
         import torch
         host_w = [w.contiguous().view(torch.int16).cpu().numpy().astype(np.uint16) for w in self.weight]
         host_w[3] = host_w[3][:TRIPLES]
@@ -176,7 +177,7 @@ class OrderModel:
             args += [w.ctypes.data_as(ctypes.c_void_p), b.ctypes.data_as(ctypes.c_void_p)]
             setattr(self, f"_keep_{len(args)}", (w, b))
         _check(lib().tdp_set_order_model(slot, *args))
-        _check(lib().tdp_enable_order_model(slot, 1 if enable else 0))
+        _check(lib().tdp_enable_order_model(slot, levels if enable else 0))
 
 
 def solution_pairs(cases: Sequence[Tuple], results) -> Tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:

@@ -2,7 +2,8 @@
 11, ratio 1.375) against the oracle's restatement of the CUDA rule, on the first 120 cases
 of the seeded stream (tests/golden/verdicts_config5.json, made by make_verdicts_config5.py).
 The engine runs them in plain order and again with an untrained order model installed,
-whose arbitrary root order must not change a verdict.  Every sequence found is replayed."""
+whose arbitrary root order, and arbitrary first-level lists, must not change a verdict.
+Every sequence found is replayed."""
 import numpy as np
 import pytest
 
@@ -24,10 +25,13 @@ def test_config5_verdicts_match_oracle_in_any_root_order(native_lib, oracle):
     try:
         inst = make_instances(cases, 11, False)
         plain = search_batch(0, inst, len(cases), R1375)
-        order_model.OrderModel().install(0, enable=True)  # random weights: an arbitrary root order
+        model = order_model.OrderModel()  # random weights: an arbitrary order
+        model.install(0, enable=True, levels=1)
         ordered = search_batch(0, inst, len(cases), R1375)
+        native_lib.tdp_enable_order_model(0, 2)
+        ordered2 = search_batch(0, inst, len(cases), R1375)
         assert native_lib.tdp_mlp_error() == 0
-        for res in (plain, ordered):
+        for res in (plain, ordered, ordered2):
             for row, case, r in zip(rows, cases, res):
                 assert r.status == row[3], row[0]
                 if r.status == 1:

@@ -146,13 +146,25 @@ def test_training_reduces_loss_and_ordering_keeps_verdicts(native_lib, torch_cud
         inst = make_instances(eval_cases, 8, False)
         plain = search_batch(0, inst, len(eval_cases), R1375)
         plain_status = [r.status for r in plain]
-        model.install(0, enable=True)
-        ordered = search_batch(0, inst, len(eval_cases), R1375)
-        assert [r.status for r in ordered] == plain_status
-        for (p, s, e), r in zip(eval_cases, ordered):
-            if r.status == 1:
-                pos = [[r.positions[3 * d + t] for t in range(3)] for d in range(r.depth)]
-                ok, _ = oracle.replay_positions(list(p), list(s), pos, e, R1375, False)
-                assert ok
+        for levels in (1, 2):
+            model.install(0, enable=True, levels=levels)
+            ordered = search_batch(0, inst, len(eval_cases), R1375)
+            assert [r.status for r in ordered] == plain_status
+            for (p, s, e), r in zip(eval_cases, ordered):
+                if r.status == 1:
+                    pos = [[r.positions[3 * d + t] for t in range(3)] for d in range(r.depth)]
+                    ok, _ = oracle.replay_positions(list(p), list(s), pos, e, R1375, False)
+                    assert ok
+        # exhaustive searches under both orders: config-1 full sorting at depth 11 (negatives
+        # dominate) must keep the fixture's verdicts with learned root and first-level order
+        from conftest import load_golden
+        rows = [r for r in load_golden("verdicts_config1.json")["cases"][:300] if r["full11"] in (0, 1)]
+        stream = list(config_cases(1, max(r["case"] for r in rows) + 1))
+        cases = [stream[r["case"]][:3] for r in rows]
+        for levels in (1, 2):
+            model.install(0, enable=True, levels=levels)
+            res = search_batch(0, make_instances(cases, 11, True), len(cases), R1375)
+            assert [r.status for r in res[:len(cases)]] == [r["full11"] for r in rows], levels
+        assert native_lib.tdp_mlp_error() == 0
     finally:
         GPUSortingSearch.destroySlots()
