@@ -64,9 +64,10 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--extras", default=",".join(EXTRAS), help="comma list of extra measurements ('' for none)")
-    p.add_argument("--workload", choices=["config2", "config1", "canonical"], default="config2",
-                   help="config1 (m~U{4,5,6}) is the small case used for profiling; canonical measures the "
-                        "batched canonical form (Configuration.getCanonical) instead of the search")
+    p.add_argument("--workload", choices=["config2", "config1", "canonical", "pi_filter"], default="config2",
+                   help="config1 (m~U{4,5,6}) is a small case for profiling; canonical measures the batched "
+                        "canonical form (Configuration.getCanonical) and pi_filter the permutation filter alone")
+    p.add_argument("--first-case", type=int, default=0, help="offset of the first case of step 0 (profiling)")
     p.add_argument("--canonical-count", type=int, default=1_000_000)
     p.add_argument("--table-entries", type=int, default=DEDUP_ENTRIES)
     p.add_argument("--table-replacement", type=int, default=2)
@@ -89,9 +90,9 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def step_cases(step: int, rank: int, world: int, batch: int, config: int = CONFIG):
+def step_cases(step: int, rank: int, world: int, batch: int, config: int = CONFIG, first: int = 0):
     from tdp1375_b200.cases import config_cases
-    start = ((step * world + rank) * batch) % TOTAL_CASES
+    start = (first + (step * world + rank) * batch) % TOTAL_CASES
     out = []
     for case in range(start, start + batch):
         c = next(config_cases(config, 1, start=case % TOTAL_CASES))
@@ -213,6 +214,10 @@ def measured_hbm():
 
 
 ENTRY_BYTES = 32.0  # one transposition-table entry (n <= 32 layout)
+# DRAM bytes (read + write) per expanded node of the search kernel at the 2M-entry table, from
+# an ncu capture of config-2 cases 4..7 (57.2 MB for 385,527 nodes); the bench scales it by
+# the nodes of its own launches, which are too long to capture whole.
+NCU_DRAM_BYTES_PER_NODE = 148.4
 TASK_BYTES = 208.0  # one donated task (written by the donor, read by the receiver)
 INSTANCE_BYTES = 144.0 + 96.0  # InstanceIn read + InstanceOut written
 
@@ -558,7 +563,7 @@ def run_ours(args):
     config_id = 1 if args.workload == "config1" else CONFIG
     flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")
     total_steps = args.warmup + args.steps
-    raw_steps = [step_cases(s, rank, world, args.batch, config_id) for s in range(total_steps)]
+    raw_steps = [step_cases(s, rank, world, args.batch, config_id, args.first_case) for s in range(total_steps)]
     batches = [make_instances([c[:3] for c in cases], MAX_DEPTH, True) for cases in raw_steps]
     rate = __import__("ctypes").c_float(float(np.float32(2) / np.float32(1.375)))
 
@@ -627,11 +632,16 @@ def run_ours(args):
         "warp_busy_frac": round(agg["busy_warp_cycles"] / max(1, agg["warp_cycles"]), 4),
         "gpu_launches": agg["launches"],
         "roofline": {"bound": "hbm", "achieved": round(achieved, 3), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 6), "traffic": None,
+                     "frac": round(achieved / peak, 6),
+                     "traffic": (round(NCU_DRAM_BYTES_PER_NODE * agg["nodes"] / launches, 1)
+                                 if args.table_entries == DEDUP_ENTRIES else None),
                      "note": f"algorithmic bytes per launch = 32 B x (table probes + inserts) + 2 x 208 B x donations "
                              f"+ 240 B x instances, over the mean launch time (CUDA events on the engine stream); "
-                             f"peak {peak_kind}; the 64 MB table of the BASELINE config stays in L2, so the "
-                             "kernel is bound by table-probe latency and L2 atomics, not HBM bandwidth (see atomics)"},
+                             f"peak {peak_kind}; traffic = DRAM bytes per launch scaled from an ncu capture "
+                             "(148 B per expanded node at the 2M-entry table) by the launch's nodes; the 64 MB "
+                             "table of the BASELINE config stays in L2, so the kernel is bound by the latency of "
+                             "its dependent L2 round trips and its register-limited warp count, not HBM bandwidth "
+                             "(ncu: issue-active 42 %, long-scoreboard stalls first; see atomics)"},
         "e2e": {"value": round(cases / wall, 3) if wall > 0 else None, "unit": "cases/s",
                 "h2d_bytes_per_step": args.batch * 144, "d2h_bytes_per_step": args.batch * 96},
         "clocks": clocks.summary(),
@@ -807,6 +817,10 @@ def main():
     args = parse_args()
     if args.workload == "canonical":
         run_canonical(args)
+    elif args.workload == "pi_filter":
+        from tdp1375_b200 import native
+        print(json.dumps({"metric": "permutation-filter candidates/s (tdp_pi_filter, n = 11 and 12)",
+                          "pi_filter": extra_pi_filter(native)}), flush=True)
     elif args.impl == "reference":
         run_reference(args)
     else:
