@@ -71,6 +71,8 @@ def parse_args():
     p.add_argument("--canonical-count", type=int, default=1_000_000)
     p.add_argument("--table-entries", type=int, default=DEDUP_ENTRIES)
     p.add_argument("--table-replacement", type=int, default=2)
+    p.add_argument("--commute", type=int, default=1, help="partial-order reduction (engine option commute)")
+    p.add_argument("--probe-leaves", type=int, default=0, help="engine option probe_leaves")
     p.add_argument("--time-limit-s", type=float, default=600.0)
     p.add_argument("--blocks-per-sm", type=int, default=0, help="engine occupancy cap (0: the kernel's maximum)")
     p.add_argument("--poll-interval", type=int, default=0, help="engine poll interval in chunks (0: the default)")
@@ -230,13 +232,16 @@ def algorithmic_bytes(probes: int, inserts: int, donations: int, instances: int)
 
 
 STAT_FIELDS = ("nodes", "children", "dedup_probes", "dedup_pruned", "dedup_inserts", "dedup_full", "dedup_replaced",
-               "table_atomics", "donations", "task_pops", "busy_warp_cycles", "warp_cycles", "launches")
+               "table_atomics", "commute_skips", "donations", "task_pops", "busy_warp_cycles", "warp_cycles",
+               "launches")
 
 
 def set_engine(api, slot, args, **overrides):
     cfg = api.engine_config(slot)
     cfg.time_limit_s = args.time_limit_s
     cfg.table_replacement = args.table_replacement
+    cfg.commute = args.commute
+    cfg.probe_leaves = args.probe_leaves
     if args.blocks_per_sm > 0:
         cfg.blocks_per_sm = args.blocks_per_sm
     if args.poll_interval > 0:
@@ -625,7 +630,8 @@ def run_ours(args):
                    "parallelism": f"replicas x{world} (cases sharded, no collective)",
                    "engine": {"blocks_per_sm": cfg.blocks_per_sm, "poll_interval": cfg.poll_interval,
                               "sparse_enumeration": cfg.sparse_enumeration, "tight_bound": cfg.tight_bound,
-                              "table_replacement": cfg.table_replacement}},
+                              "table_replacement": cfg.table_replacement, "commute": cfg.commute,
+                              "probe_leaves": cfg.probe_leaves}},
         "nodes_per_s": round(nodes / (sum(kernel_ms) / 1e3), 1),
         "verdicts": verdicts,
         "counters_per_step": {f: round(agg[f] / args.steps, 1) for f in STAT_FIELDS if f != "launches"},

@@ -147,7 +147,11 @@ typedef struct tdp_engine_config {
                                    two moves could also be made in the other order and the child's
                                    smallest symbol is the smaller (that order reaches the same state
                                    at the same depth); 0 = every child.  Verdicts are the same. */
-    int32_t reserved;
+    int32_t probe_leaves;       /* 0 (default) = a child whose own children can only be tested for
+                                   success (nothing two levels down is admitted for expansion) is
+                                   admitted without a table probe: expanding it again costs less
+                                   than the lookup; 1 = probe every admitted child, as the
+                                   reference does.  Verdicts are the same. */
 } tdp_engine_config;
 
 int tdp_get_engine_config(int slot, tdp_engine_config *cfg);
@@ -183,6 +187,19 @@ int64_t tdp_extension_filter(const uint8_t *spi, const uint8_t *pi, int n, int c
 /* Same on device buffers, on `stream`; returns 0 (the caller counts keep bytes). */
 int tdp_extension_filter_device(const uint8_t *spi, const uint8_t *pi, int n, int count, uint8_t *keep,
                                 void *stream);
+
+/* ---- extend step: one-3-cycle insertions (Extensions.java:95-141, Type 1 and Type 2) ----
+ * For `count` configurations (spi rows of 64 bytes over n[r] <= 60 symbols, pi = identity),
+ * slot e of configuration r (tdp_insertion_extension_slots(max_n) slots each, the multisets
+ * a <= b <= c over [0, max_n) in lexicographic order) inserts a new unoriented 3-cycle before
+ * old positions a, b, c.  flags[r * slots + e] = 1 for a Type 1 extension (the configuration
+ * has open gates and one of a, b, c is one), 2 for a Type 2 extension (no open gate), 0
+ * otherwise; the extended spi (n + 3 symbols) goes to out[(r * slots + e) * 64].  gates[r]
+ * receives the open-gate mask (CommonOperations.getOpenGates).  Device buffers, on `stream`. */
+int64_t tdp_insertion_extension_slots(int max_n);
+int tdp_insertion_extensions_device(const uint8_t *spi, const uint8_t *n, int count, int max_n, uint64_t *gates,
+                                    uint8_t *flags, uint8_t *out, void *stream);
+const char *tdp_insertion_extensions_error(void);
 
 /* ---- learned move ordering (no counterpart in the reference) ------------------------
  * A 1088 -> 256 -> 256 -> 256 -> 4960 BF16 MLP (fp32 accumulation on the tcgen05 tensor

@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fno-fast-math",
               "-Xcompiler", "-ffp-contract=off"]
 SOURCES = ["search_engine.cu", "pi_filter.cu", "extension_filter.cu", "canonical.cu", "mlp_gemm.cu", "mlp_kernels.cu",
-           "measure.cu", "capi.cu"]
+           "measure.cu", "insertion_extensions.cu", "capi.cu"]
 
 
 def nvcc() -> str:

@@ -215,7 +215,8 @@ int tdp_set_engine_config(int slot, const tdp_engine_config *cfg) {
     if (!s) return fail(TDP_ERR_SLOT, "invalid slot");
     if (!cfg || cfg->poll_interval <= 0 || cfg->time_limit_s <= 0 || cfg->blocks_per_sm < 0 ||
         cfg->warps_per_instance < 0 || cfg->sparse_enumeration < 0 || cfg->sparse_enumeration > 2 ||
-        cfg->table_replacement < 0 || cfg->table_replacement > 3 || cfg->commute < 0 || cfg->commute > 1)
+        cfg->table_replacement < 0 || cfg->table_replacement > 3 || cfg->commute < 0 || cfg->commute > 1 ||
+        cfg->probe_leaves < 0 || cfg->probe_leaves > 1)
         return fail(TDP_ERR_ARGUMENT, "tdp_set_engine_config: invalid configuration");
     s->setConfig(*cfg);
     return 0;

@@ -160,6 +160,7 @@ struct EngineParams {
     int replace;                     // full-window policy: 0 admit unrecorded, 1 deepest, 2 oldest,
                                      // 3 deepest then oldest (see dedup_admit)
     int commute;                     // 1: partial-order reduction of commuting moves (por_skip)
+    int probeLeaves;                 // 1: probe the table for children whose children are leaves
 };
 
 }  // namespace tdp

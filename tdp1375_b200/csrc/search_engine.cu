@@ -318,6 +318,7 @@ void SearchSlot::launchClass(int cls, int offset, int count) {
     P.order2List = kLevel1List;
     P.replace = cfg_.table_replacement;
     P.commute = cfg_.commute;
+    P.probeLeaves = cfg_.probe_leaves;
 
     int blocksPerSM = 0;
     const int threads = dev::kWarpsPerBlock * 32;

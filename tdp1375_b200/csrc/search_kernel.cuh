@@ -1083,8 +1083,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                     if (lane == 0) S.stats[kStatCommuteSkips] += (unsigned)__popc(skipped);
                     probe = probe && !skip;
                 }
+                // A child whose own children can only be tested for success (no node two levels
+                // down is admitted for expansion) is cheaper to expand again than to look up:
+                // unless probe_leaves is set it is admitted without touching the table.
+                bool leafAdmit = false;
+                if (!P.probeLeaves && (f + 2 > kMaxDepth || S.rules[16 + f + 2] == 0ull)) {
+                    leafAdmit = probe;
+                    probe = false;
+                }
                 const unsigned probing = __ballot_sync(kFull, probe);
-                uint32_t outc = 0u;
+                uint32_t outc = leafAdmit ? kAdmitted : 0u;
                 if (probe) {
                     uint64_t ck[KW];
 #pragma unroll

@@ -41,7 +41,7 @@ class EngineConfig(ctypes.Structure):
                 ("task_capacity", ctypes.c_int32), ("time_limit_s", ctypes.c_double),
                 ("sparse_enumeration", ctypes.c_int32), ("use_cuda_graph", ctypes.c_int32),
                 ("warps_per_instance", ctypes.c_int32), ("table_replacement", ctypes.c_int32),
-                ("commute", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("commute", ctypes.c_int32), ("probe_leaves", ctypes.c_int32)]
 
 
 assert ctypes.sizeof(Instance) == 136 and ctypes.sizeof(Result) == 208
@@ -92,6 +92,9 @@ SIGNATURES = {
     "tdp_measure_atomics": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int, ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_double)]),
     "tdp_measure_last_error": (ctypes.c_char_p, []),
+    "tdp_insertion_extension_slots": (ctypes.c_int64, [ctypes.c_int]),
+    "tdp_insertion_extensions_device": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]),
+    "tdp_insertion_extensions_error": (ctypes.c_char_p, []),
     "tdp_pi_filter_noalloc": (ctypes.c_int64, [u8p, ctypes.c_int, u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
                                                ctypes.c_int64, vp]),
 }

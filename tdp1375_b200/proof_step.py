@@ -18,7 +18,7 @@ import argparse
 import json
 import time
 
-from . import api, casefile, extensions, frontier
+from . import extend_gpu, api, casefile, extensions, frontier
 
 SEEDS = ["(0 3 1 4 2)", "(0 4 2)(1 5 3)", "(0 3 1)(2 5 4)"]
 
@@ -52,9 +52,10 @@ def main(argv=None):
                     found_lines.append(casefile.format_line(r.spi, r.moves))
             t1 = time.perf_counter()
             nxt = []
-            for r in bad:
-                for _, ext in (extensions.type1_extensions(r.spi) + extensions.type2_extensions(r.spi) +
-                               extensions.type3_extensions(r.spi)):
+            # Type 1/2 insertions of every bad case in one device launch; Type 3 on the host
+            inserted, _ = extend_gpu.insertion_extensions([r.spi for r in bad]) if bad else ([], [])
+            for r, ins in zip(bad, inserted):
+                for ext in [e for _, e in ins] + [e for _, e in extensions.type3_extensions(r.spi)]:
                     if len(ext) <= args.max_n:
                         nxt.append(ext)
                 if len(nxt) >= args.max_frontier:

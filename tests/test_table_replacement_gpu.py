@@ -70,3 +70,30 @@ def test_device_deadline_returns_device_error_and_slot_survives(native_lib):
     got = GPUSortingSearch.searchForSortingSeq(list(small[0]), list(small[1]), small[2], R1375, 11, True, 1)
     want = load_golden("verdicts_config1.json")["cases"][0]["full11"]
     assert (1 if got else 0) == want
+
+
+def test_engine_options_keep_config1_verdicts(native_lib, oracle):
+    """The partial-order reduction (commute) and probe-free leaf admission (probe_leaves = 0)
+    on and off, on the config-1 fixture's full-sorting and partial settings."""
+    from tdp1375_b200 import GPUSortingSearch, api, make_instances, search_batch
+    from tdp1375_b200.cases import config_cases
+    rows = load_golden("verdicts_config1.json")["cases"][:250]
+    stream = list(config_cases(1, len(rows)))
+    GPUSortingSearch(1, 1, 256 << 20, 1 << 22)
+    try:
+        for commute, probe_leaves in ((1, 0), (0, 0), (1, 1), (0, 1)):
+            _config(0, commute=commute, probe_leaves=probe_leaves)
+            for key, full, depth in (("full11", True, 11), ("partial6", False, 6)):
+                sel = [r for r in rows if r[key] in (0, 1)]
+                cases = [stream[r["case"]][:3] for r in sel]
+                res = search_batch(0, make_instances(cases, depth, full), len(cases), R1375)
+                st = api.last_stats(0)
+                assert (st.commute_skips > 0) == bool(commute) or key == "partial6"
+                for row, case, r in zip(sel, cases, res):
+                    assert r.status == row[key], (commute, probe_leaves, key, row["case"])
+                    if r.status == 1:
+                        pos = [[r.positions[3 * d + t] for t in range(3)] for d in range(r.depth)]
+                        ok, _ = oracle.replay_positions(list(case[0]), list(case[1]), pos, case[2], R1375, full)
+                        assert ok
+    finally:
+        GPUSortingSearch(1, 2, 256 << 20, 1 << 21)
