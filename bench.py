@@ -686,14 +686,16 @@ def run_ours(args):
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's CPU search (SortingSearch.java)
+    on all host cores.  Step s samples the cases of the GPU arm's step s (its first case and the
+    ones after it) for --ref-step-s seconds."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     samples = []
-    first = 0
     for s in range(args.warmup + args.steps):
+        first = (args.first_case + s * args.batch) % TOTAL_CASES
         cps, nps, cores, detail, _ = cpu_sample(args.ref_step_s, args.cpu_node_limit, first_case=first)
-        first += 4 * cores
         if s >= args.warmup:
             samples.append((cps, nps))
     value = sum(x[0] for x in samples) / len(samples)
@@ -711,8 +713,10 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "u8",
         "data": "synthetic (seeded 3-permutations, numpy PCG64)",
-        "config": {"workload": "config2: 100,000 seeded 3-permutations, m~U{4..8} (n<=24), full sorting, "
-                               "ratio 1.375, max depth 11", "parallelism": "host cores"},
+        "config": {"workload": "config2: 100,000 seeded 3-permutations, m~U{4..8} (n<=24), full sorting, ratio 1.375, "
+                               "max depth 11, 3000 MB queue budget, 1 slot",
+                   "batch_per_step": args.batch, "parallelism": "host cores",
+                   "sample": "step s starts at the first case of the GPU arm's step s"},
         "nodes_per_s": round(sum(x[1] for x in samples) / len(samples), 1),
         "cpu_baseline": {"value": round(value, 4), "unit": "cases/s", "cores": cores, "kind": "port",
                          "sample": detail},
