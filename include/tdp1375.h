@@ -254,9 +254,9 @@ int tdp_enable_order_model(int slot, int enable);
  * cudaStream_t, may be null) and the call returns when it is done, with the total number
  * of hits (rows beyond max_rows are counted but not written).  The first call on a device
  * (and the first after that device's context was reset) looks up the array's device
- * address with cudaGetSymbolAddress; make that first call before any stream capture.  All
- * calls share the one array and it keeps the last call's contents, so calls that overlap
- * on the GPU (other streams or threads at the same time) race: serialise them. */
+ * address with cudaGetSymbolAddress.  All calls share the one array and it keeps the last
+ * call's contents, so calls that overlap on the GPU (other streams or threads at the same
+ * time) race: serialise them. */
 int64_t tdp_pi_filter_noalloc(const uint8_t *cycle, int cycle_len, const uint8_t *oriented_triple, int triple_len,
                               int n, int skip_2move_check, uint8_t *out_device, int64_t max_rows, void *stream);
 

@@ -114,12 +114,14 @@ constexpr uint32_t kMaxGeneration = 4094;  // generation 4095 would collide with
 constexpr int kInstanceBits = 20;          // up to 1,048,576 instances per launch
 
 // Transposition-table entry.  key = spi packed 5 bits/symbol, 12 per word (n <= 32) or
-// 6 bits/symbol, 10 per word (n <= 63).  tag = generation << 20 | instance.
-// meta = version << 13 | epoch << 5 | best depth.  The version counts the entry's rewrites,
-// so the 64-bit header (tag, meta) read before and after a key read tells whether the key
-// belongs to the header (a seqlock: kernels may overwrite live entries of a full window).
-// The epoch is the write time in units of 2^20 ns (8 bits, so ages up to ~268 ms compare
-// correctly), used by the recency replacement policies.
+// 6 bits/symbol, 10 per word (n <= 63), in the low 60 bits of each word.
+// tag = generation << 20 | instance.  meta = version << 13 | epoch << 5 | best depth.
+// The version counts the entry's rewrites, and every key word carries the low 4 bits of the
+// version that wrote it in its top 4 bits, so one read of the header and the key words tells
+// whether the key belongs to the header: kernels may overwrite live entries of a full window,
+// and a reader that meets a key word of another version treats the entry as unknown.
+// The epoch is the write (or last useful read) time in units of 2^20 ns (8 bits, so ages up
+// to ~268 ms compare correctly), used by the recency replacement policies.
 template <int KW>
 struct alignas(KW == 3 ? 32 : 64) DedupEntry {
     uint32_t tag;
@@ -131,6 +133,8 @@ constexpr uint32_t kDepthMask = (1u << kDepthBits) - 1u;
 constexpr uint32_t kEpochShift = 5;
 constexpr uint32_t kEpochMask = 255u << kEpochShift;
 constexpr uint32_t kVersionShift = 13;
+constexpr int kKeyCheckShift = 60;  // key word bits 60..63: version & 15 of the writer
+constexpr uint64_t kKeyBits = (1ull << kKeyCheckShift) - 1ull;
 
 struct EngineParams {
     const InstanceIn *in;

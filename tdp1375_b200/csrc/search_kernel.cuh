@@ -217,7 +217,13 @@ __device__ __forceinline__ uint64_t cas_acq_rel_u64(void *p, uint64_t cmp, uint6
                  : "memory");
     return old;
 }
-__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+// A CAS whose outcome nobody reads (the epoch refresh of an entry that pruned): the warp
+// does not wait for it.
+__device__ __forceinline__ void cas_relaxed_u64_nowait(void *p, uint64_t cmp, uint64_t val) {
+    uint64_t old;
+    asm volatile("atom.relaxed.gpu.global.cas.b64 %0, [%1], %2, %3;" : "=l"(old) : "l"(p), "l"(cmp), "l"(val));
+    (void)old;
+}
 
 // Transposition-table admission (sorting_search.cu:261-298 semantics, per instance): a
 // state of the same instance admitted at a depth <= `depth` prunes it; otherwise it is
@@ -225,25 +231,28 @@ __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_re
 //
 // Entries are written under a claim: a 64-bit CAS of the header (tag, meta) from the value
 // read to (kTagWriting, version + 1 | epoch | depth) with acquire-release order, then the
-// key, then a release store of the tag.  With P.replace = 0 only empty entries and entries
-// of older generations or finished instances are claimed, so an entry that carries this
-// instance's tag is never rewritten while the instance runs: a key read after the tag is
-// that entry's key, and best depths only decrease.  With P.replace > 0 a full window also
-// claims one of its live entries (policy 1: the deepest, if at least as deep as the
-// newcomer; 2: the oldest; 3: the deepest, the oldest among those), so a key read may race
-// with a rewrite.  A prune then counts only if the header read again after the key (behind
-// a fence) is unchanged: the rewrite's claim changes the header before any key store, and
-// the version never repeats.  A depth improvement is a CAS of the header read, which also
-// fails after a rewrite.  A failed check admits the child, which only costs work.
+// key words, each tagged with (version + 1) & 15 in its top 4 bits, then a release store of
+// the tag.  With P.replace = 0 only empty entries and entries of older generations or
+// finished instances are claimed; with P.replace > 0 a full window also claims one of its
+// live entries (policy 1: the deepest, if at least as deep as the newcomer; 2: the oldest;
+// 3: the deepest, the oldest among those), so a key read may race with a rewrite.
+// A reader loads the window's eight headers, then, without a fence, the key words of the
+// entries that carry its tag.  An entry matches when every key word equals the child's key
+// and carries the version of the header read: such words were all written by that
+// version's writer, which published that tag, unless the entry was rewritten a multiple of
+// 16 times between the two loads, each rewrite needing a header read and a CAS on the
+// entry after the previous one's release.  A key word of another version (a rewrite in
+// flight, or a store not yet visible) makes the entry unknown: the child is admitted
+// without an entry, which only costs work.  A depth improvement is a CAS of the header
+// read, which fails after a rewrite.  With the recency policies (2, 3) a prune also moves
+// the entry's epoch to now, so entries that keep pruning outlive entries nobody meets.
 template <int KW>
 __device__ __forceinline__ uint32_t dedup_admit(const EngineParams &P, uint32_t generation, uint32_t tag,
                                             const uint64_t (&key)[KW], uint64_t h, uint32_t depth) {
     auto *table = reinterpret_cast<DedupEntry<KW> *>(P.table);
     const uint32_t base = (uint32_t)(h >> 24) & P.tableMask & ~7u;
     const uint32_t epoch = (uint32_t)(global_time_ns() >> 20) & 255u;
-    // Eight independent relaxed header loads (one round trip); only when a tag matches does
-    // the lane pay an acquire fence before reading keys, which pairs with the release store
-    // that published the entry.
+    // Eight independent relaxed header loads (one round trip).
     uint64_t hdr[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) hdr[q] = ld_relaxed_u64(&table[base + q]);
@@ -260,17 +269,22 @@ __device__ __forceinline__ uint32_t dedup_admit(const EngineParams &P, uint32_t 
         }
     }
     if (tagMask) {
-        fence_acq_rel_gpu();
-        // the keys of every entry with this instance's tag, loaded together
-        unsigned eqMask = 0;
+        // the key words of every entry with this instance's tag, loaded together
+        unsigned eqMask = 0, unknownMask = 0;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             if ((tagMask >> q) & 1u) {
                 const DedupEntry<KW> *e = &table[base + q];
-                bool eq = true;
+                const uint64_t check = (uint64_t)(((uint32_t)(hdr[q] >> 32) >> kVersionShift) & 15u) << kKeyCheckShift;
+                bool eq = true, other = false;
 #pragma unroll
-                for (int kq = 0; kq < KW; ++kq) eq &= (ld_relaxed_u64(&e->key[kq]) == key[kq]);
-                eqMask |= (eq ? 1u : 0u) << q;
+                for (int kq = 0; kq < KW; ++kq) {
+                    const uint64_t v = ld_relaxed_u64(&e->key[kq]);
+                    eq &= (v & kKeyBits) == key[kq];
+                    other |= (v & ~kKeyBits) != check;
+                }
+                eqMask |= (eq && !other ? 1u : 0u) << q;
+                unknownMask |= (other ? 1u : 0u) << q;
             }
         }
         if (eqMask) {
@@ -283,8 +297,9 @@ __device__ __forceinline__ uint32_t dedup_admit(const EngineParams &P, uint32_t 
             const uint32_t mm = (uint32_t)(hm >> 32);
             if (P.replace) {
                 if ((mm & kDepthMask) <= depth) {
-                    fence_acq_rel_gpu();
-                    return ld_relaxed_u64(e) == hm ? 0u : kAdmitted;
+                    if (P.replace >= 2 && ((mm & kEpochMask) >> kEpochShift) != epoch)
+                        cas_relaxed_u64_nowait(e, hm, ((uint64_t)((mm & ~kEpochMask) | (epoch << kEpochShift)) << 32) | tag);
+                    return 0u;
                 }
                 const uint32_t nm = (mm & ~(kDepthMask | kEpochMask)) | (epoch << kEpochShift) | depth;
                 cas_acq_rel_u64(e, hm, ((uint64_t)nm << 32) | tag);
@@ -296,6 +311,7 @@ __device__ __forceinline__ uint32_t dedup_admit(const EngineParams &P, uint32_t 
             const uint32_t prev = atomicMin(&e->meta, (mm & ~kDepthMask) | depth);
             return (prev & kDepthMask) <= depth ? kAtomic : (kAdmitted | kAtomic);
         }
+        if (unknownMask) return kAdmitted;
         liveMask |= tagMask;
     }
     if (freeMask == 0u) {
@@ -349,7 +365,9 @@ __device__ __forceinline__ uint32_t dedup_admit(const EngineParams &P, uint32_t 
         ((uint64_t)((version << kVersionShift) | (epoch << kEpochShift) | depth) << 32) | kTagWriting;
     if (cas_acq_rel_u64(e, old, claim) != old) return kAdmitted | kAtomic;
 #pragma unroll
-    for (int kq = 0; kq < KW; ++kq) st_relaxed_u64(&e->key[kq], key[kq]);
+    const uint64_t check = (uint64_t)(version & 15u) << kKeyCheckShift;
+#pragma unroll
+    for (int kq = 0; kq < KW; ++kq) st_relaxed_u64(&e->key[kq], key[kq] | check);
     st_release_u32(&e->tag, tag);  // the release orders the key stores before it
     return outcome | kAtomic;
 }
