@@ -633,6 +633,7 @@ def run_ours(args):
                               "table_replacement": cfg.table_replacement, "commute": cfg.commute,
                               "probe_leaves": cfg.probe_leaves}},
         "nodes_per_s": round(nodes / (sum(kernel_ms) / 1e3), 1),
+        "step_ms": [round(x, 1) for x in kernel_ms],
         "verdicts": verdicts,
         "counters_per_step": {f: round(agg[f] / args.steps, 1) for f in STAT_FIELDS if f != "launches"},
         "warp_busy_frac": round(agg["busy_warp_cycles"] / max(1, agg["warp_cycles"]), 4),
