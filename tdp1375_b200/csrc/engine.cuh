@@ -162,7 +162,7 @@ struct EngineParams {
     int order2Ranks, order2List;
     int maxInFlight;                 // admitted-but-unfinished instance cap (0 = none)
     int replace;                     // full-window policy: 0 admit unrecorded, 1 deepest, 2 oldest,
-                                     // 3 deepest then oldest (see dedup_admit)
+                                     // 3 deepest then oldest (see dedup_admit_warp)
     int commute;                     // 1: partial-order reduction of commuting moves (por_skip)
     int probeLeaves;                 // 1: probe the table for children whose children are leaves
 };

@@ -196,7 +196,7 @@ __device__ __forceinline__ uint64_t key_hash(const uint64_t (&k)[KW], uint32_t t
     return h;
 }
 
-// Outcome bits of dedup_admit: admitted, inserted into an empty, reclaimed or replaced
+// Outcome bits of dedup_admit_warp: admitted, inserted into an empty, reclaimed or replaced
 // entry, admitted without an entry because the window was full, inserted over a live entry
 // of a full window, and "issued an atomic" (a claim or a depth update, for the statistics).
 constexpr uint32_t kAdmitted = 1u, kInserted = 2u, kWindowFull = 4u, kReplaced = 8u, kAtomic = 16u;
@@ -229,147 +229,175 @@ __device__ __forceinline__ void cas_relaxed_u64_nowait(void *p, uint64_t cmp, ui
 // state of the same instance admitted at a depth <= `depth` prunes it; otherwise it is
 // admitted and recorded.
 //
+// The warp probes together: every round takes up to four of the chunk's children, and the
+// eight lanes of group g read the eight entries of child g's window, each lane one whole
+// entry (header and key words in 16-byte loads), so a window costs one round trip and a
+// prune needs no other.  The group decides from its ballots; one lane of the group then
+// issues the group's only atomic, and the outcome goes back to the child's lane.
+//
 // Entries are written under a claim: a 64-bit CAS of the header (tag, meta) from the value
 // read to (kTagWriting, version + 1 | epoch | depth) with acquire-release order, then the
 // key words, each tagged with (version + 1) & 15 in its top 4 bits, then a release store of
 // the tag.  With P.replace = 0 only empty entries and entries of older generations or
-// finished instances are claimed; with P.replace > 0 a full window also claims one of its
-// live entries (policy 1: the deepest, if at least as deep as the newcomer; 2: the oldest;
-// 3: the deepest, the oldest among those), so a key read may race with a rewrite.
-// A reader loads the window's eight headers, then, without a fence, the key words of the
-// entries that carry its tag.  An entry matches when every key word equals the child's key
-// and carries the version of the header read: such words were all written by that
-// version's writer, which published that tag, unless the entry was rewritten a multiple of
-// 16 times between the two loads, each rewrite needing a header read and a CAS on the
-// entry after the previous one's release.  A key word of another version (a rewrite in
-// flight, or a store not yet visible) makes the entry unknown: the child is admitted
-// without an entry, which only costs work.  A depth improvement is a CAS of the header
-// read, which fails after a rewrite.  With the recency policies (2, 3) a prune also moves
-// the entry's epoch to now, so entries that keep pruning outlive entries nobody meets.
+// finished instances are claimed; with P.replace > 0 a full window claims one of its live
+// entries instead (policy 1: the deepest, if at least as deep as the newcomer; 2: the
+// oldest; 3: the deepest, the oldest among those), so a key read may race with a rewrite.
+// An entry matches when it carries the instance's tag and every key word equals the
+// child's key and carries the version of the header read: such words were all written by
+// that version's writer, which published that tag, unless the entry was rewritten a
+// multiple of 16 times between the loads of one round, each rewrite needing a header read
+// and a CAS on the entry after the previous one's release.  A key word of another version
+// (a rewrite in flight, or a store not yet visible) makes the entry unknown: the child is
+// admitted without an entry, which only costs work.  A depth improvement is a CAS of the
+// header read, which fails after a rewrite.  With the recency policies (2, 3) a prune also
+// moves the entry's epoch to now, so entries that keep pruning outlive entries nobody meets.
+// Two children of one round that share a window may pick the same entry; the losing CAS
+// admits its child without an entry.
 template <int KW>
-__device__ __forceinline__ uint32_t dedup_admit(const EngineParams &P, uint32_t generation, uint32_t tag,
-                                            const uint64_t (&key)[KW], uint64_t h, uint32_t depth) {
+__device__ __forceinline__ void load_entry(const DedupEntry<KW> *e, uint64_t &hdr, uint64_t (&kw)[KW]) {
+    const uint64_t *p = reinterpret_cast<const uint64_t *>(e);
+    uint64_t v[KW + 1];
+#pragma unroll
+    for (int t = 0; t < (KW + 1) / 2; ++t)
+        asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];"
+                     : "=l"(v[2 * t]), "=l"(v[2 * t + 1])
+                     : "l"(p + 2 * t));
+    hdr = v[0];
+#pragma unroll
+    for (int kq = 0; kq < KW; ++kq) kw[kq] = v[kq + 1];
+}
+
+// All lanes call it with the ballot `todo` of the lanes that probe; returns the outcome bits
+// of the calling lane's own child (0 for a lane not in todo).
+template <int KW>
+__device__ __forceinline__ uint32_t dedup_admit_warp(const EngineParams &P, uint32_t generation, uint32_t tag,
+                                                     unsigned todo, const uint64_t (&key)[KW], uint64_t h,
+                                                     uint32_t depth, int lane) {
     auto *table = reinterpret_cast<DedupEntry<KW> *>(P.table);
-    const uint32_t base = (uint32_t)(h >> 24) & P.tableMask & ~7u;
+    const uint32_t myBase = (uint32_t)(h >> 24) & P.tableMask & ~7u;
     const uint32_t epoch = (uint32_t)(global_time_ns() >> 20) & 255u;
-    // Eight independent relaxed header loads (one round trip).
-    uint64_t hdr[8];
+    const int grp = lane >> 3, q = lane & 7, sh = grp * 8;
+    uint32_t mine = 0u;
+    while (todo) {
+        // this round: the first four children of todo, the g-th for group g
+        unsigned rest = todo;
+        int src = -1;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) hdr[q] = ld_relaxed_u64(&table[base + q]);
-    unsigned tagMask = 0, freeMask = 0, liveMask = 0;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const uint32_t t = (uint32_t)hdr[q];
-        if (t == tag) {
-            tagMask |= 1u << q;
-        } else if (t == 0u || (t != kTagWriting && (t >> kInstanceBits) != generation)) {
-            freeMask |= 1u << q;
-        } else if (t != kTagWriting) {
-            liveMask |= 1u << q;
+        for (int g = 0; g < 4; ++g) {
+            const int b = rest ? __ffs(rest) - 1 : -1;
+            if (g == grp) src = b;
+            rest &= rest - 1u;
         }
-    }
-    if (tagMask) {
-        // the key words of every entry with this instance's tag, loaded together
-        unsigned eqMask = 0, unknownMask = 0;
+        const unsigned round = todo & ~rest;
+        todo = rest;
+        const bool active = src >= 0;
+        const int s = active ? src : lane;
+        const uint32_t base = __shfl_sync(kFull, myBase, s);
+        uint64_t k[KW];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            if ((tagMask >> q) & 1u) {
-                const DedupEntry<KW> *e = &table[base + q];
-                const uint64_t check = (uint64_t)(((uint32_t)(hdr[q] >> 32) >> kVersionShift) & 15u) << kKeyCheckShift;
-                bool eq = true, other = false;
+        for (int kq = 0; kq < KW; ++kq) k[kq] = shfl64(key[kq], s);
+        DedupEntry<KW> *e = &table[base + q];
+        uint64_t hd = 0ull, kw[KW];
 #pragma unroll
-                for (int kq = 0; kq < KW; ++kq) {
-                    const uint64_t v = ld_relaxed_u64(&e->key[kq]);
-                    eq &= (v & kKeyBits) == key[kq];
-                    other |= (v & ~kKeyBits) != check;
-                }
-                eqMask |= (eq && !other ? 1u : 0u) << q;
-                unknownMask |= (other ? 1u : 0u) << q;
+        for (int kq = 0; kq < KW; ++kq) kw[kq] = 0ull;
+        if (active) load_entry<KW>(e, hd, kw);
+        const uint32_t t = (uint32_t)hd, mm = (uint32_t)(hd >> 32);
+        const uint64_t check = (uint64_t)((mm >> kVersionShift) & 15u) << kKeyCheckShift;
+        bool eq = true, other = false;
+#pragma unroll
+        for (int kq = 0; kq < KW; ++kq) {
+            eq &= (kw[kq] & kKeyBits) == k[kq];
+            other |= (kw[kq] & ~kKeyBits) != check;
+        }
+        const bool isTag = active && t == tag;
+        const bool isFree = active && (t == 0u || (t != kTagWriting && (t >> kInstanceBits) != generation));
+        const bool isLive = active && !isTag && !isFree && t != kTagWriting;
+        const unsigned e8 = (__ballot_sync(kFull, isTag && eq && !other) >> sh) & 0xFFu;
+        const unsigned u8 = (__ballot_sync(kFull, isTag && other) >> sh) & 0xFFu;
+        unsigned f8 = (__ballot_sync(kFull, isFree) >> sh) & 0xFFu;
+        const unsigned l8 = (__ballot_sync(kFull, isLive || (isTag && !eq && !other)) >> sh) & 0xFFu;
+        const bool insertPath = active && e8 == 0u && u8 == 0u;
+        if (!P.replace && __any_sync(kFull, insertPath && f8 == 0u)) {
+            // no empty or old-generation entry: entries of finished instances are free too
+            bool done = false;
+            if (insertPath && f8 == 0u && ((l8 >> q) & 1u)) {
+                const uint32_t idx = t & ((1u << kInstanceBits) - 1u);
+                done = (ld_relaxed_u32(P.doneBits + (idx >> 5)) >> (idx & 31u)) & 1u;
             }
+            f8 |= (__ballot_sync(kFull, done) >> sh) & 0xFFu;
         }
-        if (eqMask) {
-            const int m = __ffs(eqMask) - 1;
-            uint64_t hm = 0;
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-                if (q == m) hm = hdr[q];
-            DedupEntry<KW> *e = &table[base + m];
-            const uint32_t mm = (uint32_t)(hm >> 32);
-            if (P.replace) {
-                if ((mm & kDepthMask) <= depth) {
-                    if (P.replace >= 2 && ((mm & kEpochMask) >> kEpochShift) != epoch)
-                        cas_relaxed_u64_nowait(e, hm, ((uint64_t)((mm & ~kEpochMask) | (epoch << kEpochShift)) << 32) | tag);
-                    return 0u;
-                }
-                const uint32_t nm = (mm & ~(kDepthMask | kEpochMask)) | (epoch << kEpochShift) | depth;
-                cas_acq_rel_u64(e, hm, ((uint64_t)nm << 32) | tag);
-                return kAdmitted | kAtomic;
-            }
-            // Best depths only decrease, so a header value that is already <= depth decides
-            // the prune without an atomic.
-            if ((mm & kDepthMask) <= depth) return 0u;
-            const uint32_t prev = atomicMin(&e->meta, (mm & ~kDepthMask) | depth);
-            return (prev & kDepthMask) <= depth ? kAtomic : (kAdmitted | kAtomic);
-        }
-        if (unknownMask) return kAdmitted;
-        liveMask |= tagMask;
-    }
-    if (freeMask == 0u) {
-        // No empty or old-generation entry: entries of finished instances are free too
-        // (their done bits, loaded together).
-        uint32_t done[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const uint32_t idx = (uint32_t)hdr[q] & ((1u << kInstanceBits) - 1u);
-            done[q] = ((liveMask >> q) & 1u) ? ld_relaxed_u32(P.doneBits + (idx >> 5)) : 0u;
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const uint32_t idx = (uint32_t)hdr[q] & ((1u << kInstanceBits) - 1u);
-            if ((done[q] >> (idx & 31u)) & 1u) freeMask |= 1u << q;
-        }
-    }
-    int slot = freeMask ? (__ffs(freeMask) - 1) : -1;
-    uint32_t outcome = kAdmitted | kInserted;
-    if (slot < 0) {
-        if (!P.replace) return kAdmitted | kWindowFull;
-        // The victim: policy 1 the deepest live entry at least as deep as the newcomer
-        // (shallow entries prune the largest subtrees); 2 the oldest live entry; 3 the
-        // deepest, the oldest among equally deep ones.  Ties go to the later slot.
-        uint32_t best = 0;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const uint32_t m = (uint32_t)(hdr[q] >> 32);
-            const uint32_t d = m & kDepthMask;
-            const uint32_t age = (epoch - ((m & kEpochMask) >> kEpochShift)) & 255u;
-            const uint32_t score = P.replace == 1 ? (d >= depth ? d + 1u : 0u)
+        // the victim of a full window (P.replace > 0): the highest score, ties to the later
+        // slot; score 0 = not a candidate
+        uint32_t pick = 0u;
+        if (P.replace && __any_sync(kFull, insertPath && f8 == 0u)) {
+            const uint32_t d = mm & kDepthMask;
+            const uint32_t age = (epoch - ((mm & kEpochMask) >> kEpochShift)) & 255u;
+            const uint32_t score = !((l8 >> q) & 1u) ? 0u
+                                   : P.replace == 1 ? (d >= depth ? d + 1u : 0u)
                                    : P.replace == 2 ? age + 1u
                                                     : ((d << 8) | age) + 1u;
-            if (((liveMask >> q) & 1u) && score >= best && score > 0u) {
-                best = score;
-                slot = q;
+            pick = (score << 3) | (uint32_t)q;
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) pick = max(pick, __shfl_xor_sync(kFull, pick, o));
+        }
+        // the group's decision, taken by one lane of the group
+        uint32_t res = 0u;
+        bool claim = false, improve = false;
+        uint64_t casNew = 0ull;
+        if (active) {
+            if (e8) {
+                if (q == __ffs(e8) - 1) {
+                    if ((mm & kDepthMask) <= depth) {
+                        if (P.replace >= 2 && ((mm & kEpochMask) >> kEpochShift) != epoch)
+                            cas_relaxed_u64_nowait(e, hd,
+                                                   ((uint64_t)((mm & ~kEpochMask) | (epoch << kEpochShift)) << 32) | tag);
+                    } else if (P.replace) {
+                        improve = true;
+                        casNew = ((uint64_t)((mm & ~(kDepthMask | kEpochMask)) | (epoch << kEpochShift) | depth) << 32) |
+                                 tag;
+                        res = kAdmitted | kAtomic;
+                    } else {
+                        // best depths only decrease while the instance runs (no rewrite of its
+                        // live entries without replacement)
+                        const uint32_t prev = atomicMin(&e->meta, (mm & ~kDepthMask) | depth);
+                        res = (prev & kDepthMask) <= depth ? kAtomic : (kAdmitted | kAtomic);
+                    }
+                }
+            } else if (u8) {
+                if (q == 0) res = kAdmitted;
+            } else {
+                const int slot = f8 ? __ffs(f8) - 1 : ((pick >> 3) ? (int)(pick & 7u) : -1);
+                if (slot < 0) {
+                    if (q == 0) res = kAdmitted | kWindowFull;
+                } else if (q == slot) {
+                    claim = true;
+                    const uint32_t version = (mm >> kVersionShift) + 1u;
+                    casNew = ((uint64_t)((version << kVersionShift) | (epoch << kEpochShift) | depth) << 32) | kTagWriting;
+                    res = kAdmitted | kInserted | (f8 ? 0u : kReplaced) | kAtomic;
+                }
             }
         }
-        if (slot < 0) return kAdmitted | kWindowFull;
-        outcome |= kReplaced;
+        if (claim || improve) {
+            const uint64_t got = cas_acq_rel_u64(e, hd, casNew);
+            if (claim) {
+                if (got == hd) {
+                    const uint64_t nib = (uint64_t)((((mm >> kVersionShift) + 1u) & 15u)) << kKeyCheckShift;
+#pragma unroll
+                    for (int kq = 0; kq < KW; ++kq) st_relaxed_u64(&e->key[kq], k[kq] | nib);
+                    st_release_u32(&e->tag, tag);  // the release orders the key stores before it
+                } else {
+                    res = kAdmitted | kAtomic;
+                }
+            }
+        }
+        // the group's outcome to every lane of the group, then to the child's lane
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) res |= __shfl_xor_sync(kFull, res, o);
+        const int rank = __popc(round & ((1u << lane) - 1u));
+        const uint32_t got = __shfl_sync(kFull, res, (rank & 3) * 8);
+        if ((round >> lane) & 1u) mine = got;
     }
-    // an unrolled select keeps the headers in registers (a dynamic index would put them in
-    // local memory on every probe)
-    uint64_t old = 0;
-#pragma unroll
-    for (int q = 0; q < 8; ++q)
-        if (q == slot) old = hdr[q];
-    DedupEntry<KW> *e = &table[base + slot];
-    const uint32_t version = ((uint32_t)(old >> 32) >> kVersionShift) + 1u;
-    const uint64_t claim =
-        ((uint64_t)((version << kVersionShift) | (epoch << kEpochShift) | depth) << 32) | kTagWriting;
-    if (cas_acq_rel_u64(e, old, claim) != old) return kAdmitted | kAtomic;
-#pragma unroll
-    const uint64_t check = (uint64_t)(version & 15u) << kKeyCheckShift;
-#pragma unroll
-    for (int kq = 0; kq < KW; ++kq) st_relaxed_u64(&e->key[kq], key[kq] | check);
-    st_release_u32(&e->tag, tag);  // the release orders the key stores before it
-    return outcome | kAtomic;
+    return mine;
 }
 
 // Partial-order reduction of commuting moves (verdict-preserving; no counterpart in the
@@ -1111,14 +1139,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, NW == 1 ? 4 : 2) search_e
                 }
                 const unsigned probing = __ballot_sync(kFull, probe);
                 uint32_t outc = leafAdmit ? kAdmitted : 0u;
-                if (probe) {
+                if (probing) {
                     uint64_t ck[KW];
 #pragma unroll
                     for (int q = 0; q < KW; ++q) ck[q] = key[q];
                     set_field<NW>(ck, a, w_spi(wc));
                     set_field<NW>(ck, b, w_spi(wa));
                     set_field<NW>(ck, c, w_spi(wb));
-                    outc = dedup_admit<KW>(P, generation, tag, ck, key_hash<KW>(ck, tag), (uint32_t)(f + 1));
+                    const uint32_t r =
+                        dedup_admit_warp<KW>(P, generation, tag, probing, ck, key_hash<KW>(ck, tag), (uint32_t)(f + 1), lane);
+                    if (probe) outc = r;
                 }
                 pending = __ballot_sync(kFull, outc & kAdmitted);
                 const unsigned atomics = __ballot_sync(kFull, outc & kAtomic);
