@@ -217,9 +217,9 @@ def measured_hbm():
 
 ENTRY_BYTES = 32.0  # one transposition-table entry (n <= 32 layout)
 # DRAM bytes (read + write) per expanded node of the search kernel at the 2M-entry table, from
-# an ncu capture of config-2 cases 4..7 (57.2 MB for 385,527 nodes); the bench scales it by
+# an ncu capture of config-2 cases 96..99 (2.69 GB for 72.8 M nodes); the bench scales it by
 # the nodes of its own launches, which are too long to capture whole.
-NCU_DRAM_BYTES_PER_NODE = 148.4
+NCU_DRAM_BYTES_PER_NODE = 36.9
 TASK_BYTES = 208.0  # one donated task (written by the donor, read by the receiver)
 INSTANCE_BYTES = 144.0 + 96.0  # InstanceIn read + InstanceOut written
 
@@ -645,10 +645,11 @@ def run_ours(args):
                      "note": f"algorithmic bytes per launch = 32 B x (table probes + inserts) + 2 x 208 B x donations "
                              f"+ 240 B x instances, over the mean launch time (CUDA events on the engine stream); "
                              f"peak {peak_kind}; traffic = DRAM bytes per launch scaled from an ncu capture "
-                             "(148 B per expanded node at the 2M-entry table) by the launch's nodes; the 64 MB "
-                             "table of the BASELINE config stays in L2, so the kernel is bound by the latency of "
-                             "its dependent L2 round trips and its register-limited warp count, not HBM bandwidth "
-                             "(ncu: issue-active 42 %, long-scoreboard stalls first; see atomics)"},
+                             "(37 B per expanded node at the 2M-entry table, mostly write-backs of spilled "
+                             "registers) by the launch's nodes; the 64 MB table of the BASELINE config stays in L2, "
+                             "so the kernel is bound by instruction issue and dependent latency (ncu: 2,452 warp "
+                             "instructions per node at 57 % issue; stalls: instruction fetch, shuffle chains, table "
+                             "round trips), not HBM bandwidth; see atomics"},
         "e2e": {"value": round(cases / wall, 3) if wall > 0 else None, "unit": "cases/s",
                 "h2d_bytes_per_step": args.batch * 144, "d2h_bytes_per_step": args.batch * 96},
         "clocks": clocks.summary(),

@@ -124,7 +124,7 @@ int tdp_last_stats(int slot, tdp_stats *out);
 
 typedef struct tdp_engine_config {
     int32_t blocks_per_sm;   /* 0 = occupancy maximum */
-    int32_t poll_interval;   /* chunks between flag polls / donation checks (default 32) */
+    int32_t poll_interval;   /* chunks between flag polls / donation checks (default 64) */
     int32_t tight_bound;     /* 1 = verdict-preserving strengthened prune, 0 = reference prune only */
     int32_t task_capacity;   /* read-only: warp mailboxes for work donation (sized from the queue budget) */
     double time_limit_s;     /* device deadline per launch */

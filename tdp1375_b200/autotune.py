@@ -30,7 +30,7 @@ CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotune_cache
 
 DEFAULT_SPACE = {
     "blocks_per_sm": [0, 2, 1],
-    "poll_interval": [4, 8, 16, 32],
+    "poll_interval": [8, 16, 32, 64],
     "sparse_enumeration": [2, 1],
 }
 

@@ -102,7 +102,7 @@ private:
     std::vector<int> order_;
     int count_ = 0, countSmall_ = 0;
 
-    tdp_engine_config cfg_{0, 32, 1, 0, 120.0, 2, 0, 0, 2, 1, 0};
+    tdp_engine_config cfg_{0, 64, 1, 0, 120.0, 2, 0, 0, 2, 1, 0};
     unsigned long long statsAccum_[kStatCount] = {};
     double kernelMs_ = 0.0;
     int deviceError_ = 0;
