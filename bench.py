@@ -340,7 +340,11 @@ def extra_learned(args, api, native):
         native.load().tdp_enable_order_model(0, 0)
         return {"model": "1088-256-256-256-4960 BF16 MLP, tcgen05 GEMMs; 'learned' reorders each root's children, "
                          "'learned_two_levels' also the children of each root's 16 best children",
-                "training": {"pairs": int(len(tgt)), "pair_generation_s": round(t_pairs, 2),
+                "training": {"instances": "3-permutations with m in 4..6 (config-1 sizes) and 8..10, partial mode, "
+                                          "depth 11, from seeds disjoint from both samples (the m = 8..10 half "
+                                          "lets the model see the evaluation's sizes; BASELINE's pairs come from "
+                                          "config 1 alone)",
+                             "pairs": int(len(tgt)), "pair_generation_s": round(t_pairs, 2),
                              "train_s": round(t_train, 2), "steps": tstats.steps,
                              "loss": [round(tstats.first_loss, 3), round(tstats.last_loss, 3)]},
                 "samples": samples,
