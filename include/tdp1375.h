@@ -138,8 +138,9 @@ typedef struct tdp_engine_config {
                                    0 = admit it without recording, as sorting_search.cu:291-297;
                                    1 = overwrite the deepest entry if it is at least as deep;
                                    2 = overwrite the oldest entry; 3 = overwrite the deepest
-                                   entry, the oldest among equally deep ones.  Verdicts are the
-                                   same under every policy; the default is 2 (on a table far
+                                   entry, the oldest among equally deep ones.  Under 2 and 3 an
+                                   entry that prunes a state counts as new again.  Verdicts are
+                                   the same under every policy; the default is 2 (on a table far
                                    smaller than a search's states, recency keeps the duplicates
                                    that nearby subtrees produce). */
     int32_t commute;            /* 1 (default) = partial-order reduction: a child move on symbols
