@@ -651,9 +651,9 @@ def run_ours(args):
                              f"peak {peak_kind}; traffic = DRAM bytes per launch scaled from an ncu capture "
                              "(37 B per expanded node at the 2M-entry table, mostly write-backs of spilled "
                              "registers) by the launch's nodes; the 64 MB table of the BASELINE config stays in L2, "
-                             "so the kernel is bound by instruction issue and dependent latency (ncu: 2,452 warp "
-                             "instructions per node at 57 % issue; stalls: instruction fetch, shuffle chains, table "
-                             "round trips), not HBM bandwidth; see atomics"},
+                             "so the kernel is bound by instruction issue and dependent latency (ncu on the headline's "
+                             "last step: 57 % issue; stalls: instruction fetch, shuffle chains, table round trips), "
+                             "not HBM bandwidth; see atomics"},
         "e2e": {"value": round(cases / wall, 3) if wall > 0 else None, "unit": "cases/s",
                 "h2d_bytes_per_step": args.batch * 144, "d2h_bytes_per_step": args.batch * 96},
         "clocks": clocks.summary(),
