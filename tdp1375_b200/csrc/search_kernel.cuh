@@ -8,14 +8,17 @@
 //     can_still_reach and the transposition table admits it (sorting_search.cu:562-563);
 //   * the transposition table prunes a state only when the same state of the same
 //     instance was admitted at a depth <= the current one (sorting_search.cu:261-298);
-//     a full probe window admits without inserting.
+//     a full probe window admits without inserting (table_replacement 0), or recycles
+//     one of its live entries (policies 1-3), which only changes the work.
 // Layout differences (B200-first, not a translation):
-//   * one warp runs a lazy DFS: a node's children are evaluated 32 at a time (one
-//     lexicographic triple per lane), admitted children are kept as a 32-bit pending
-//     mask and descended into one by one; the frame stack (<= 16 frames) lives in
-//     shared memory (per-lane symbol words) and in lane-indexed registers (frame f's
-//     cursor/mask/key live in lane f), so no node is ever copied through global memory
-//     except when work is donated;
+//   * one warp runs a lazy DFS: a node's children are evaluated 32 at a time (one triple
+//     per lane: lexicographic, or only the same-cycle pairs/triples that can help),
+//     admitted children are kept as a 32-bit pending mask and descended into one by one;
+//     the frame stack (<= 16 frames) lives in shared memory (per-lane symbol words and one
+//     record per frame), so no node is ever copied through global memory except when work
+//     is donated;
+//   * the warp probes the table together: eight lanes read one child's eight-entry window,
+//     header and key words at once (dedup_admit_warp);
 //   * each lane owns one symbol/position word (spi, pi, cycle leader, steps to leader,
 //     cycle length) so a child's odd-cycle count is an O(1) delta (tdp_math.cuh) instead
 //     of an O(n) recount, and a descent rebuilds the cycle tables with pointer jumping
