@@ -412,9 +412,11 @@ __device__ __forceinline__ uint32_t dedup_admit_warp(const EngineParams &P, uint
 // reaches the same state at the same depth through the kept order.  Every admission
 // condition of the rule tables is monotone along a move sequence (a move changes the
 // odd-cycle count by at most 2), so the kept order passes them wherever the skipped one
-// does; a state's subtree is explored from its first admission, and any child that
-// admission skips is reached through its parent's commuted sibling, by induction on depth
-// and then on the move order.
+// does.  With the transposition table a state is expanded only at its admissions; a child
+// skipped at one is reached through the parent's commuted sibling, whose admission may skip
+// the (larger) incoming move in turn, and so on: the least symbol of the last move grows
+// strictly along that chain, so by induction on depth every reachable state is admitted at
+// a depth no larger than its own.
 __device__ __forceinline__ bool por_skip(uint32_t inc, uint32_t x, uint32_t y, uint32_t z, uint32_t i, uint32_t j,
                                          uint32_t k, uint32_t a, uint32_t b, uint32_t c) {
     if (a == x || a == y || a == z || b == x || b == y || b == z || c == x || c == y || c == z) return false;
