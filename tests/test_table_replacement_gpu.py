@@ -1,7 +1,8 @@
 """A transposition table far smaller than the searches need must give the verdicts of the
 fixtures under every full-window policy (tdp_engine_config.table_replacement): admit
 without recording, as sorting_search.cu:291-297 does, or overwrite a live entry (the
-deepest, the oldest, or the oldest of the deepest) with seqlock-validated reads.  Also: the per-launch device
+deepest, the oldest, or the oldest of the deepest) while other warps read it, their key
+reads validated by the version carried in each key word.  Also: the per-launch device
 deadline ends a long search with TDP_ERR_DEVICE and leaves the slot usable."""
 import numpy as np
 import pytest
